@@ -1,0 +1,188 @@
+"""ctypes bindings of the two CPU oracles.
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline / reference legs, never by the product.
+
+* :func:`run_oracle`  — oracle/build/libthy_oracle.so, the FP64 restatement
+  of the time stepper (thy_oracle.c), fed with in-memory inputs.
+* :func:`run_refemu`  — oracle/_ref/librefemu.so, the reference's own
+  kernels, loader and NetCDF writers compiled for the host; it reads the
+  problem files from disk exactly as the reference's main() does.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from typing import Dict, Optional
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "build", "libthy_oracle.so")
+REFEMU_SO = os.path.join(HERE, "_ref", "librefemu.so")
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+
+
+class _Problem(ctypes.Structure):
+    _fields_ = [
+        ("nx", ctypes.c_int), ("ny", ctypes.c_int),
+        ("lon", _f64p), ("lat", _f64p), ("z", _f32p), ("eta_file", _f32p),
+        ("nfaults", ctypes.c_int), ("faults", _f64p),
+        ("crop_flag", ctypes.c_int), ("crop_value", ctypes.c_double),
+        ("borders", ctypes.c_double * 4),
+        ("sim_time", ctypes.c_double), ("save_time", ctypes.c_double), ("series_time", ctypes.c_double),
+        ("npoints", ctypes.c_int), ("points", _f64p),
+        ("cfl", ctypes.c_double), ("eps_h", ctypes.c_double), ("hpos", ctypes.c_double),
+        ("stability", ctypes.c_double), ("manning", ctypes.c_double), ("vmax", ctypes.c_double),
+        ("L", ctypes.c_double), ("H", ctypes.c_double), ("dif_at", ctypes.c_double),
+        ("max_iterations", ctypes.c_longlong), ("threads", ctypes.c_int),
+    ]
+
+
+class _Result(ctypes.Structure):
+    _fields_ = [
+        ("max_height", _f32p), ("arrival", _f32p), ("deformed_bathy", _f32p),
+        ("eta", _f32p), ("ux", _f32p), ("uy", _f32p),
+        ("max_snaps", ctypes.c_int), ("snap_eta", _f32p), ("snap_ux", _f32p), ("snap_uy", _f32p),
+        ("snap_time", _f64p), ("nsnaps", ctypes.c_int),
+        ("max_series", ctypes.c_int), ("ts_eta", _f32p), ("ts_ux", _f32p), ("ts_uy", _f32p),
+        ("ts_time", _f64p), ("ts_min", _f32p), ("ts_max", _f32p), ("ts_bathy", _f32p),
+        ("nseries", ctypes.c_int), ("npoints_unique", ctypes.c_int),
+        ("iterations", ctypes.c_longlong), ("final_time", ctypes.c_double),
+        ("first_dt", ctypes.c_double), ("loop_seconds", ctypes.c_double),
+    ]
+
+
+_lib = None
+_ref = None
+
+
+def oracle_lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            raise RuntimeError(f"oracle library missing: {ORACLE_SO} (run `make -C oracle`)")
+        _lib = ctypes.CDLL(ORACLE_SO)
+        _lib.thy_oracle_run.argtypes = [ctypes.POINTER(_Problem), ctypes.POINTER(_Result)]
+        _lib.thy_oracle_run.restype = ctypes.c_int
+        _lib.thy_oracle_okada_points.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p, _f64p]
+    return _lib
+
+
+def refemu_available() -> bool:
+    return os.path.exists(REFEMU_SO)
+
+
+def refemu_lib():
+    global _ref
+    if _ref is None:
+        if not refemu_available():
+            raise RuntimeError(f"ref-emu library missing: {REFEMU_SO} (run `make -C oracle ref`)")
+        _ref = ctypes.CDLL(REFEMU_SO)
+        _ref.refemu_run.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _f64p]
+        _ref.refemu_run.restype = ctypes.c_int
+        _ref.refemu_okada_points.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p, _f64p]
+    return _ref
+
+
+def _ptr(a: Optional[np.ndarray], ctype):
+    if a is None:
+        return ctypes.cast(None, ctype)
+    return a.ctypes.data_as(ctype)
+
+
+def run_oracle(p, max_iterations: int = -1, threads: int = 0, max_snaps: int = 0, max_series: int = 0) -> Dict:
+    """Runs the FP64 oracle on a thysea.synth.Problem; returns numpy fields."""
+    lib = oracle_lib()
+    nx, ny = p.nx, p.ny
+    lon = np.ascontiguousarray(p.lon, dtype=np.float64)
+    lat = np.ascontiguousarray(p.lat, dtype=np.float64)
+    z = np.ascontiguousarray(p.z, dtype=np.float32)
+    eta_file = None if p.faults else np.ascontiguousarray(
+        np.zeros_like(z) if p.eta_init is None else p.eta_init, dtype=np.float32)
+    faults = np.ascontiguousarray(p.fault_array(), dtype=np.float64) if p.faults else None
+    pts = None if p.points is None else np.ascontiguousarray(p.points, dtype=np.float64)
+    pr = _Problem()
+    pr.nx, pr.ny = nx, ny
+    pr.lon, pr.lat, pr.z = _ptr(lon, _f64p), _ptr(lat, _f64p), _ptr(z, _f32p)
+    pr.eta_file = _ptr(eta_file, _f32p)
+    pr.nfaults = len(p.faults)
+    pr.faults = _ptr(faults, _f64p)
+    pr.crop_flag, pr.crop_value = int(p.crop_flag), float(p.crop_value)
+    for i in range(4):
+        pr.borders[i] = float(p.borders[i])
+    pr.sim_time, pr.save_time = float(p.sim_time), float(p.save_time)
+    pr.series_time = float(p.series_time) if pts is not None else -1.0
+    pr.npoints = 0 if pts is None else len(pts)
+    pr.points = _ptr(pts, _f64p)
+    pr.cfl, pr.eps_h, pr.hpos, pr.stability = p.cfl, p.eps_h, p.hpos, p.stability
+    pr.manning, pr.vmax, pr.L, pr.H, pr.dif_at = p.manning, p.vmax, p.L, p.H, p.dif_at
+    pr.max_iterations = max_iterations
+    pr.threads = threads
+    out = {k: np.empty((ny, nx), np.float32) for k in ("max_height", "arrival", "deformed_bathy", "eta", "ux", "uy")}
+    npts = 0 if pts is None else len(pts)
+    snaps = {k: np.empty((max(max_snaps, 1), ny, nx), np.float32) for k in ("snap_eta", "snap_ux", "snap_uy")}
+    snap_time = np.empty(max(max_snaps, 1), np.float64)
+    ser = {k: np.empty((max(max_series, 1), max(npts, 1)), np.float32) for k in ("ts_eta", "ts_ux", "ts_uy")}
+    ts_time = np.empty(max(max_series, 1), np.float64)
+    ts_pts = {k: np.empty(max(npts, 1), np.float32) for k in ("ts_min", "ts_max", "ts_bathy")}
+    r = _Result()
+    for k, v in out.items():
+        setattr(r, k, _ptr(v, _f32p))
+    r.max_snaps = max_snaps
+    for k, v in snaps.items():
+        setattr(r, k, _ptr(v, _f32p))
+    r.snap_time = _ptr(snap_time, _f64p)
+    r.max_series = max_series
+    for k, v in ser.items():
+        setattr(r, k, _ptr(v, _f32p))
+    r.ts_time = _ptr(ts_time, _f64p)
+    for k, v in ts_pts.items():
+        setattr(r, k, _ptr(v, _f32p))
+    rc = lib.thy_oracle_run(ctypes.byref(pr), ctypes.byref(r))
+    if rc != 0:
+        raise RuntimeError(f"thy_oracle_run failed: {rc}")
+    res = dict(out)
+    ns = min(r.nsnaps, max_snaps)
+    res["snapshots"] = {"eta": snaps["snap_eta"][:ns], "ux": snaps["snap_ux"][:ns], "uy": snaps["snap_uy"][:ns],
+                        "time": snap_time[:ns]}
+    nt, nu = min(r.nseries, max_series), r.npoints_unique
+    res["series"] = {"eta": ser["ts_eta"][:nt, :nu], "ux": ser["ts_ux"][:nt, :nu], "uy": ser["ts_uy"][:nt, :nu],
+                     "time": ts_time[:nt], "min": ts_pts["ts_min"][:nu], "max": ts_pts["ts_max"][:nu],
+                     "bathy": ts_pts["ts_bathy"][:nu]}
+    res.update(iterations=r.iterations, final_time=r.final_time, first_dt=r.first_dt,
+               loop_seconds=r.loop_seconds, nsnaps=r.nsnaps, nseries=r.nseries)
+    return res
+
+
+def oracle_okada_points(lon, lat, fault_row) -> np.ndarray:
+    lib = oracle_lib()
+    lon = np.ascontiguousarray(lon, np.float64)
+    lat = np.ascontiguousarray(lat, np.float64)
+    f = np.ascontiguousarray(fault_row, np.float64)
+    out = np.empty_like(lon)
+    lib.thy_oracle_okada_points(len(lon), _ptr(lon, _f64p), _ptr(lat, _f64p), _ptr(f, _f64p), _ptr(out, _f64p))
+    return out
+
+
+def refemu_okada_points(lon, lat, fault_row) -> np.ndarray:
+    lib = refemu_lib()
+    lon = np.ascontiguousarray(lon, np.float64)
+    lat = np.ascontiguousarray(lat, np.float64)
+    f = np.ascontiguousarray(fault_row, np.float64)
+    out = np.empty_like(lon)
+    lib.refemu_okada_points(len(lon), _ptr(lon, _f64p), _ptr(lat, _f64p), _ptr(f, _f64p), _ptr(out, _f64p))
+    return out
+
+
+def run_refemu(txt_path: str, max_iterations: int = -1, threads: int = 0, quiet: bool = True) -> Dict:
+    """Runs the reference's own code (compiled for the host) on a problem
+    file; the outputs are the NetCDF files named by the file's prefix."""
+    lib = refemu_lib()
+    info = (ctypes.c_double * 4)()
+    rc = lib.refemu_run(txt_path.encode(), max_iterations, threads, 1 if quiet else 0, info)
+    if rc != 0:
+        raise RuntimeError(f"refemu_run failed: {rc}")
+    return {"iterations": int(info[0]), "final_time": info[1], "loop_seconds": info[2], "first_dt": info[3]}

@@ -1,0 +1,70 @@
+/*
+ * thy_oracle — FP64 CPU restatement of the Tsunami-HySEA time stepper.
+ *
+ * TEST INFRASTRUCTURE.  Only tests/, __graft_entry__.smoke() and bench.py's
+ * CPU-baseline leg load this library, and only as the checker / CPU
+ * baseline.  The product (tsunami-hysea_b200/) never links or calls it.
+ *
+ * Inputs are exactly what the reference's problem file and its GRD /
+ * points files carry (dimensional: degrees, metres, seconds); the oracle
+ * performs the reference loader's nondimensionalisation itself.
+ */
+#ifndef THY_ORACLE_H
+#define THY_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int nx, ny;
+    const double *lon;        /* nx, degrees */
+    const double *lat;        /* ny, degrees */
+    const float *z;           /* ny*nx topobathymetry, metres, positive up */
+    const float *eta_file;    /* ny*nx initial sea surface (m); NULL = Okada initialisation */
+    int nfaults;
+    const double *faults;     /* nfaults*10: time lon lat depth_km length_km width_km strike dip rake slip_m */
+    int crop_flag;            /* 0 none, 1 relative, 2 absolute */
+    double crop_value;
+    double borders[4];        /* upper, lower, left, right: 1 open, -1 wall, 2 periodic (left/right) */
+    double sim_time, save_time, series_time; /* seconds; < 0 disables saving */
+    int npoints;
+    const double *points;     /* npoints*2 (lon, lat) as listed in the points file */
+    double cfl, eps_h, hpos, stability, manning, vmax, L, H, dif_at;
+    long long max_iterations; /* < 0: run to sim_time */
+    int threads;              /* <= 0: OpenMP default */
+} thy_oracle_problem;
+
+typedef struct {
+    /* fields, ny*nx each, may be NULL */
+    float *max_height;        /* m, -9999 where never wet */
+    float *arrival;           /* s, -1 where never reached */
+    float *deformed_bathy;    /* m, positive down */
+    float *eta, *ux, *uy;     /* final state, extracted like a snapshot */
+    /* snapshots (max_snaps*ny*nx each, may be NULL) */
+    int max_snaps;
+    float *snap_eta, *snap_ux, *snap_uy;
+    double *snap_time;        /* max_snaps */
+    int nsnaps;
+    /* time series (max_series*npoints each) */
+    int max_series;
+    float *ts_eta, *ts_ux, *ts_uy;
+    double *ts_time;
+    float *ts_min, *ts_max, *ts_bathy; /* npoints */
+    int nseries, npoints_unique;
+    /* run summary */
+    long long iterations;
+    double final_time, first_dt, loop_seconds;
+} thy_oracle_result;
+
+int thy_oracle_run(const thy_oracle_problem *p, thy_oracle_result *r);
+
+/* Okada vertical seafloor displacement (m) at n (lon, lat) points for one
+ * fault (10 values as in thy_oracle_problem.faults). */
+void thy_oracle_okada_points(int n, const double *lon, const double *lat, const double *fault, double *uz);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
