@@ -1,0 +1,169 @@
+/*
+ * thysea.h — C ABI of the B200 Tsunami-HySEA time stepper (libthysea.so).
+ *
+ * The boundary this library replaces is the reference's single plug point
+ *   extern "C" int shallowWater(...)          src/GPU/ShallowWater.cu:182-190
+ * called once by main() (src/ShallowWater.cxx:146-151) with the
+ * dimensionless problem produced by cargarDatosProblema()
+ * (src/Problema.cxx:176-477).  That symbol is exported unchanged (see
+ * thysea_dropin.h); this header is the same contract over plain C types:
+ *
+ *   thy_problem   the arguments of shallowWater() (dimensionless arrays in
+ *                 the reference's layout) gathered in one struct;
+ *   thy_outputs   where the results go (host buffers and callbacks, instead
+ *                 of the NetCDF files shallowWater() writes itself);
+ *   thy_run       the time loop of shallowWater() on the GPU.
+ *
+ * Plus the pieces around it that a caller of the reference gets from its
+ * main(): the problem-file loader (thy_load_problem_file), the
+ * nondimensionalisation (thy_prepare), and the NetCDF writers
+ * (thy_write_netcdf), and the batched / serving entry points that run many
+ * scenarios in one persistent launch (thy_batch_*, thy_server_*).
+ *
+ * Return codes 1 and 2 keep the meaning shallowWater() gives them
+ * (src/GPU/ShallowWater.cu:262-353).
+ */
+#ifndef THYSEA_H
+#define THYSEA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define THY_OK 0
+#define THY_ERR_GPU_MEMORY 1   /* not enough GPU memory (shallowWater() returns 1) */
+#define THY_ERR_HOST 2         /* host memory or output file (shallowWater() returns 2) */
+#define THY_ERR_INVALID 3      /* invalid argument or problem file */
+#define THY_ERR_CUDA 4         /* CUDA runtime error */
+#define THY_ERR_NO_DEVICE 5    /* no CUDA device (main() prints "There is no graphics card") */
+#define THY_ERR_NONFINITE 6    /* the state or the time step became non-finite */
+#define THY_ERR_BUDGET 7       /* a scenario does not fit the server's HBM budget */
+#define THY_ERR_CANCELLED 8    /* a served request was cancelled */
+
+/* ------------------------------------------------------------------------
+ * Raw problem: the contents of the problem .txt file and of its GRD and
+ * points files, in their own units (degrees, metres, seconds).
+ * Grammar: src/Problema.cxx:219-343; formats: README.md "File formats".
+ * ---------------------------------------------------------------------- */
+typedef struct thy_raw {
+    int nx, ny;
+    const double *lon;        /* nx */
+    const double *lat;        /* ny */
+    const float *z;           /* ny*nx topobathymetry, metres, positive up */
+    const float *eta_file;    /* ny*nx initial surface (m); NULL selects Okada initialisation */
+    int nfaults;
+    const double *faults;     /* nfaults*10: time(s) lon lat depth(km) length(km) width(km) strike dip rake slip(m) */
+    int crop_flag;            /* 0 none, 1 relative, 2 absolute */
+    double crop_value;
+    double borders[4];        /* upper, lower, left, right: 1 open, -1 wall, 2 periodic (left/right) */
+    double sim_time, save_time, series_time;   /* seconds; < 0 disables */
+    int npoints;
+    const double *points;     /* npoints*2 lon lat, duplicates allowed (dropped as the reference does) */
+    double cfl, eps_h, hpos, stability, manning, vmax, L, H, dif_at;
+} thy_raw;
+
+/* ------------------------------------------------------------------------
+ * Dimensionless problem: the arguments of shallowWater().
+ * ---------------------------------------------------------------------- */
+typedef struct thy_problem {
+    int nx, ny;
+    const double *h;          /* nx*ny water depth           (datosVolumenesNivel_1[i].x) */
+    const double *Hs;         /* nx*ny depth shifted by Hmin (datosVolumenesNivel_1[i].y) */
+    const double *qx;         /* nx*ny discharges (datosVolumenesNivel_2[i].x), NULL = 0 */
+    const double *qy;         /*                  (datosVolumenesNivel_2[i].y), NULL = 0 */
+    const double *area_cos;   /* ny*2: cell area, cos(lat)   (datosNivel.areaYCosPhi) */
+    const double *dlon;       /* ny+1                         (datosNivel.anchoVolumenes) */
+    const double *dlat;       /* ny                           (datosNivel.altoVolumenes) */
+    const double *lon;        /* nx degrees                   (datosNivel.longitud) */
+    const double *lat;        /* ny degrees                   (datosNivel.latitud) */
+    double Hmin;
+    double border_up, border_low, border_left, border_right;
+    int sponge_up, sponge_low, sponge_left, sponge_right;
+    double t_end, save_nc, save_ts;   /* dimensionless; save_* < 0 disables */
+    double cfl, mf0, vmax, eps_h, hpos, cvis, dif_at;
+    double L, H, Q, T;                /* scales */
+    int okada_flag;                   /* 1: faults below; 0: initial state from file (already in h) */
+    int nfaults;
+    const double *faults;             /* nfaults*10, sorted by time, as in thy_raw */
+    int crop_flag;
+    double crop_value;                /* dimensionless for absolute cropping */
+    int npoints;
+    const int *point_cell;            /* npoints cell indices (-1: outside the grid) */
+    const double *point_lon;          /* npoints gauge longitudes (lonPuntos) */
+    const double *point_lat;          /* npoints gauge latitudes  (latPuntos) */
+    long long max_steps;              /* < 0: run to t_end */
+} thy_problem;
+
+/* Snapshot / gauge callbacks: fields are dimensional float arrays laid out
+ * like the reference's NetCDF variables (eta, ux, uy: ny*nx; gauges:
+ * npoints each).  `index` counts from 0, time is in seconds. */
+typedef void (*thy_field_fn)(void *user, int index, double time_s, const float *eta, const float *ux, const float *uy);
+
+typedef struct thy_outputs {
+    float *max_height;        /* ny*nx, m, -9999 never wet         (may be NULL) */
+    float *arrival;           /* ny*nx, s, -1 never reached         (may be NULL) */
+    float *deformed_bathy;    /* ny*nx, m, positive down            (may be NULL) */
+    float *eta, *ux, *uy;     /* ny*nx final state like a snapshot  (may be NULL) */
+    float *series_min, *series_max, *series_bathy;   /* npoints      (may be NULL) */
+    thy_field_fn on_snapshot; /* called at every snapshot time     (may be NULL) */
+    thy_field_fn on_series;   /* called at every gauge time        (may be NULL) */
+    void *user;
+} thy_outputs;
+
+typedef struct thy_stats {
+    long long steps;          /* time steps taken */
+    double final_time_s;      /* simulated time reached */
+    double first_dt_s;        /* initial dt after fault-time truncation */
+    double loop_seconds;      /* wall time of the time loop (the reference's "Runtime") */
+    double device_loop_ms;    /* device time of the stepping kernels (CUDA events) */
+    long long kernel_launches;/* kernels launched by the time loop */
+    int snapshots, series_samples;
+} thy_stats;
+
+/* Library / device. */
+const char *thy_version(void);
+const char *thy_strerror(int code);
+int thy_device_count(void);                       /* 0 when no CUDA device is usable */
+int thy_set_device(int device);
+
+/* Problem set-up: file loader (problem .txt + GRD + points, the grammar of
+ * src/Problema.cxx:176-343) into a raw problem owned by the library, and the
+ * nondimensionalisation of src/Problema.cxx:319-477 into an owned problem. */
+typedef struct thy_raw_owned thy_raw_owned;
+int thy_load_problem_file(const char *txt_path, thy_raw_owned **out);
+const thy_raw *thy_raw_view(const thy_raw_owned *r);
+const char *thy_raw_name(const thy_raw_owned *r);     /* problem name (first line) */
+const char *thy_raw_bathy_file(const thy_raw_owned *r);
+const char *thy_raw_prefix(const thy_raw_owned *r);   /* NetCDF output prefix */
+void thy_raw_free(thy_raw_owned *r);
+
+typedef struct thy_problem_owned thy_problem_owned;
+int thy_prepare(const thy_raw *raw, thy_problem_owned **out);
+const thy_problem *thy_problem_view(const thy_problem_owned *p);
+void thy_problem_free(thy_problem_owned *p);
+
+/* The time loop of shallowWater() on the GPU (device 0 or thy_set_device). */
+int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *stats);
+
+/* Same problem through the reference's NetCDF outputs: <prefix>.nc and,
+ * with gauges, <prefix>_ts.nc (src/GPU/netcdfTH.cu, src/GPU/netcdfSeries.cu). */
+int thy_run_netcdf(const thy_problem *p, const char *problem_name, const char *prefix, thy_stats *stats);
+
+/* Step-level access for benchmarking: set up a problem on the device, run
+ * `steps` time steps (Okada applied first), report the device time of the
+ * stepping kernels.  No outputs are produced. */
+typedef struct thy_session thy_session;
+int thy_session_open(const thy_problem *p, thy_session **out);
+int thy_session_steps(thy_session *s, long long steps, double *device_ms, long long *steps_done);
+int thy_session_fetch(thy_session *s, float *max_height, float *eta, float *ux, float *uy);
+double thy_session_time(const thy_session *s);    /* simulated time (s) */
+void thy_session_close(thy_session *s);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* THYSEA_H */

@@ -1,0 +1,466 @@
+// Device-side data structures and FP32 edge-flux arithmetic of the B200
+// time stepper.
+//
+// State of one scenario in HBM (all FP32, row-major with a padded pitch):
+//   eta[2]  free-surface elevation above the undisturbed sea level (m / H)
+//   dep     still-water depth, positive down, Okada-deformed (m / H);
+//           water depth h = eta + dep (h = 0 exactly on dry cells: eta = -dep)
+//   qx[2], qy[2]  discharges (x: along longitude, y: along latitude)
+//   eta_max, arr, eta_ini   max-height / arrival-time diagnostics
+// eta and q are double-buffered: phase 1 reads eta[p] and writes eta[p^1],
+// phase 2 reads eta[p^1], q[p] and writes q[p^1]; the controller flips p.
+//
+// Storing eta instead of h keeps ~1e-10 resolution on the wave itself
+// (h ~ 4 in units of H would quantise the surface to ~0.5 mm); every place
+// where the reference forms a surface difference from h - H uses eta.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace thy {
+
+constexpr float kEps = 2.220446049250313e-16f;  // the reference's EPSILON (DBL_EPSILON)
+constexpr float kSqrt2 = 1.41421356237309505f;
+constexpr int kSponge = 4;
+
+// scenario status (ScenarioCtl::status)
+enum : int {
+    kRunning = 0,
+    kPaused = 1,   // an event (fault, snapshot, gauge sample) is due at time t
+    kDone = 2,     // t >= t_end or the step budget is used
+    kFailed = 3,   // non-finite state or time step
+    kIdle = 4,     // slot not in use / not started
+};
+
+// pause reasons (bit mask, ScenarioCtl::events)
+enum : int { kEvFault = 1, kEvSnapshot = 2, kEvSeries = 4, kEvStepBudget = 8 };
+
+struct RowMetrics {
+    // per row y (ny entries unless noted), FP64 on the host, rounded once
+    const float *cosphi;     // cos(lat)
+    const float *ilcos;      // x-edge length / cos(lat)  (dlat / cos)
+    const float *area;       // cell area
+    const float *dlon;       // y-edge length at edge row y (ny+1 entries); sponge dx
+    const float *dlat;       // sponge dy
+};
+
+// Mutable per-scenario control block; written by the host between graph
+// launches and by the last tile of each phase-2 launch.
+struct ScenarioCtl {
+    double t;            // simulated time (dimensionless)
+    double dt;           // time step of the next step
+    double t_end;
+    double save_nc, next_nc;   // snapshot interval / next snapshot time (< 0: off)
+    double save_ts, next_ts;   // gauge interval / next gauge time
+    double T;                  // time scale (s)
+    long long step;            // completed steps
+    long long max_steps;       // < 0: unlimited
+    int status;
+    int events;
+    int parity;
+    int fault_next;            // index of the next fault to apply
+    int jumping;               // the reference's saltar_deformacion
+    int nfaults;
+    unsigned int dt_bits;      // atomicMin target (positive float bits)
+    unsigned int tiles_done;   // phase-2 tiles finished this step
+    unsigned int errors;       // non-finite values seen
+    int pad_;
+    const double *fault_times; // nfaults fault times (s), sorted, device memory
+};
+
+struct ScenarioDev {
+    int nx, ny, pitch;
+    int tiles_x, tiles_y, ntiles;
+    int periodic;
+    float b_up, b_low, b_left, b_right;
+    int sp_up, sp_low, sp_left, sp_right;
+    float cfl, eps_h, hpos, cvis, mf0, vmax, dif_at, sea;
+    double eps_h64;   // eps_h in double for the FP64 set-up / output thresholds
+    float *eta[2];
+    float *qx[2];
+    float *qy[2];
+    float *dep;
+    float *eta_max;
+    float *arr;
+    float *eta_ini;
+    RowMetrics row;
+    ScenarioCtl *ctl;
+};
+
+__host__ __device__ inline float fmax_(float a, float b) { return (a < b) ? b : a; }
+__host__ __device__ inline float fmin_(float a, float b) { return (b < a) ? b : a; }
+
+__device__ __forceinline__ float sgnf(float a) { return (a > 0.f) ? 1.f : ((a < 0.f) ? -1.f : 0.f); }
+__device__ __forceinline__ float pow4f(float a) { float b = a * a; return b * b; }
+
+// Desingularised 1/h (src/GPU/Arista_kernel.cu:164): sqrt2 h / sqrt(h^4 + max(h,eps)^4),
+// which is exactly 1/h for h >= eps.
+__device__ __forceinline__ float inv_depth(float h, float eps)
+{
+    if (h >= eps) return __frcp_rn(h);
+    return kSqrt2 * h * rsqrtf(pow4f(h) + pow4f(eps));
+}
+
+// Monotone limiter of the WAF correction (src/GPU/Arista_kernel.cu:45-68).
+__device__ __forceinline__ float monotone_limiter(float pm, float p0, float p1, float pp, float wave)
+{
+    float d_mid = p1 - p0;
+    float d_up = (wave < 0.f) ? (pp - p1) : ((wave > 0.f) ? (p0 - pm) : 0.5f * (pp - pm));
+    float same = (d_mid * d_up >= 0.f) ? 1.f : 0.f;
+    d_mid = fabsf(d_mid);
+    d_up = fabsf(d_up);
+    if (d_mid < kEps) return 1.f;
+    float a = fabsf(__fdividef(d_up - d_mid, d_up + d_mid));
+    d_up = 0.5f * (d_up + d_mid) * (1.f - a * a * a);
+    float r = (d_mid > d_up) ? __fdividef(d_up, d_mid + kEps) : __fdividef(d_mid, d_up + kEps);
+    return same * r * __fdividef(1.f + r, 1.f + r * r);
+}
+
+// Limits a mass flux so that neither side loses more than 1/4 of its water in
+// one step (src/GPU/Arista_kernel.cu:79-114; c0/c1 = cos(lat) for y edges).
+__device__ __forceinline__ float limit_outflow(float F, float h0, float h1, float c0, float c1, float dt, float a0, float a1)
+{
+    float dt0 = (F > 0.f) ? 0.25f * h0 * c0 * a0 / (F + kEps) : 0.25f * h1 * c1 * a1 / (-F + kEps);
+    if (dt > dt0) F *= dt0 / (dt + kEps);
+    return F;
+}
+
+// Blend weight of the 2s flux against the WAF flux (src/GPU/Arista_kernel.cu:208).
+__device__ __forceinline__ float blend_2s(float hij, float hpos, bool no_lim)
+{
+    if (no_lim) return 0.f;
+    if (hij < hpos) return __frcp_rn(1.f + __expf(-15.f * (1.f - 0.5f * hpos / (hij + kEps))));
+    return 1.f;
+}
+
+// Surface-gradient term max(eta1+Hm,0) - max(eta0+Hm,0) with Hm = min(D0,D1),
+// evaluated as eta1 - eta0 whenever both sides are wet at the lower bed so that
+// FP32 does not lose the wave to the depth's magnitude.
+__device__ __forceinline__ float surface_jump(float e0, float e1, float D0, float D1)
+{
+    float Hm = fmin_(D0, D1);
+    float a = e1 + Hm, b = e0 + Hm;
+    if (a > 0.f && b > 0.f) return e1 - e0;
+    return fmax_(a, 0.f) - fmax_(b, 0.f);
+}
+
+// One edge: four stencil cells along the edge normal.  "u" is the momentum
+// component normal to the edge, "v" the tangential one.
+struct Edge {
+    float h0m, h0, h1, h1p;
+    float e0m, e0, e1, e1p;
+    float D0, D1;
+    float u0m, u0, u1, u1p;
+    float v0m, v0, v1, v1p;
+    float area0, area1, cos0, cos1;
+    float len;      // x edges: len/cos (ilcos); y edges: len
+    float normal;
+    bool front;     // ghost on the low side: sides swapped, flux computed mirrored
+    bool no_lim;    // within two cells of a boundary: first order, no 2s blend
+};
+
+__device__ __forceinline__ void swapf(float &a, float &b) { float t = a; a = b; b = t; }
+
+__device__ __forceinline__ void swap_sides(Edge &e)
+{
+    swapf(e.h0m, e.h1p); swapf(e.h0, e.h1);
+    swapf(e.e0m, e.e1p); swapf(e.e0, e.e1);
+    swapf(e.D0, e.D1);
+    swapf(e.u0m, e.u1p); swapf(e.u0, e.u1);
+    swapf(e.v0m, e.v1p); swapf(e.v0, e.v1);
+    swapf(e.area0, e.area1); swapf(e.cos0, e.cos1);
+}
+
+__device__ __forceinline__ bool all_deep(const Edge &e, float hpos)
+{
+    return (e.h0 > hpos) && (e.h1 > hpos) && (e.h0m > hpos) && (e.h1p > hpos) && !e.no_lim;
+}
+
+// ---------------------------------------------------------------------------
+// phase 1: mass flux through one edge (src/GPU/Arista_kernel.cu:118-219 for
+// x edges, 674-778 for y edges).  Returns F; the caller applies it as
+// cell0 -= F (/cos0 for y), cell1 += F (/cos1).
+// ---------------------------------------------------------------------------
+template <bool LAT>
+__device__ __forceinline__ float mass_flux(Edge &e, const ScenarioDev &s, float dt)
+{
+    if (all_deep(e, s.hpos)) {
+        if (!LAT) return limit_outflow(e.u0 * e.len, e.h0, e.h1, 1.f, 1.f, dt, e.area0, e.area1);
+        return limit_outflow(e.len * e.u0 * e.cos0, e.h0, e.h1, e.cos0, e.cos1, dt, e.area0, e.area1);
+    }
+    if (e.front) swap_sides(e);
+    const float h0 = e.h0, h1 = e.h1;
+    if (!((h0 > kEps) || (h1 > kEps))) return 0.f;
+    float q0n = e.u0 * e.normal, q1n = e.u1 * e.normal;
+    const float hij = 0.5f * (h0 + h1);
+    const float c0 = sqrtf(hij);
+    if ((h0 < s.eps_h) && (-e.e1 > e.D0)) q1n = 0.f;
+    if ((h1 < s.eps_h) && (-e.e0 > e.D1)) q0n = 0.f;
+    const float u0n = inv_depth(h0, s.eps_h) * q0n;
+    const float u1n = inv_depth(h1, s.eps_h) * q1n;
+    q0n = u0n * h0;
+    q1n = u1n * h1;
+    const float F2s = LAT ? e.len * q0n * e.cos0 * e.normal : e.len * q0n * e.normal;
+    const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+    const float uijn = (s0 * u0n + s1 * u1n) / (s0 + s1 + kEps);
+    const float val = (2.f * e.len * dt) / (e.area0 + e.area1);
+    const float aut1 = fmin_(uijn - c0, u0n - s0);
+    const float aut2 = fmax_(uijn + c0, u1n + s1);
+    const float maxa = fmax_(fabsf(aut2), fabsf(aut1));
+    float xiL = 0.f, xiR = 0.f;
+    if (!e.no_lim) {
+        xiL = monotone_limiter(e.e0m, e.e0, e.e1, e.e1p, aut1);
+        xiR = monotone_limiter(e.e0m, e.e0, e.e1, e.e1p, aut2);
+    }
+    float a0;
+    if (fabsf(aut1 - aut2) >= kEps) {
+        const float alr = sgnf(aut1) * (1.f - xiL) + val * aut1 * xiL;
+        const float blr = sgnf(aut2) * (1.f - xiR) + val * aut2 * xiR;
+        a0 = (alr - blr) * (aut1 * aut2) / (aut2 - aut1);
+    } else {
+        a0 = maxa;
+    }
+    const float jump = surface_jump(e.e0, e.e1, e.D0, e.D1);
+    float Fwaf;
+    if (!LAT) {
+        Fwaf = 0.5f * (q1n + q0n - a0 * jump) * e.len;
+    } else {
+        const float deta = 0.5f * (e.cos0 + e.cos1) * jump - uijn * uijn * (e.cos1 - e.cos0);
+        Fwaf = 0.5f * (q0n * e.cos0 + q1n * e.cos1 - a0 * deta) * e.len;
+    }
+    const float alfa = blend_2s(hij, s.hpos, e.no_lim);
+    const float F = alfa * F2s + (1.f - alfa) * Fwaf;
+    if (!LAT) return limit_outflow(F, h0, h1, 1.f, 1.f, dt, e.area0, e.area1);
+    return limit_outflow(F, h0, h1, e.cos0, e.cos1, dt, e.area0, e.area1);
+}
+
+// Result of a momentum flux: contributions to the two cells (already with
+// the "acc -= F" sign applied) and the wave-speed term for the time step.
+struct MomFlux {
+    float m_x, m_y;   // to cell0: subtract
+    float p_x, p_y;   // to cell1: subtract
+    float lam;        // edge length * max wave speed (added to both)
+    bool active;
+};
+
+// ---------------------------------------------------------------------------
+// phase 2: momentum flux of an x edge (src/GPU/Arista_kernel.cu:221-464).
+// Components are (qx, qy).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ MomFlux momentum_flux_x(Edge &e, const ScenarioDev &s, float dt)
+{
+    MomFlux r;
+    r.active = true;
+    const float ilcos = e.len;
+    if (all_deep(e, s.hpos)) {
+        const float h0 = e.h0, h1 = e.h1, hij = 0.5f * (h0 + h1);
+        const float u0n = __fdividef(e.u0, h0), u1n = __fdividef(e.u1, h1);
+        const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+        const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
+        const float maxa = fabsf(uijn) + sqrtf(hij);
+        const float jump = surface_jump(e.e0, e.e1, e.D0, e.D1);
+        float mx, my, px, py;
+        if (uijn < 0.f) {
+            mx = u1n * e.u1 * ilcos; px = -mx; mx += hij * jump * ilcos;
+            my = u1n * e.v1 * ilcos; py = -my;
+        } else {
+            mx = u0n * e.u0 * ilcos; px = -mx; mx += hij * jump * ilcos;
+            my = u0n * e.v0 * ilcos; py = -my;
+        }
+        const float cd = 0.5f * (1.f - s.cvis);
+        const float val = (2.f * ilcos * dt) / (e.area0 + e.area1);
+        const float des = cd * val * maxa * maxa * (e.u1 - e.u0) * ilcos;
+        r.m_x = mx - des; r.m_y = my;
+        r.p_x = px + des; r.p_y = py;
+        r.lam = ilcos * maxa;
+        return r;
+    }
+    if (e.front) swap_sides(e);
+    const float h0 = e.h0, h1 = e.h1;
+    if (!((h0 > kEps) || (h1 > kEps))) { r.active = false; return r; }
+    float w0 = e.u0 * e.normal, w1 = e.u1 * e.normal;
+    const float hij = 0.5f * (h0 + h1);
+    if ((h0 < s.eps_h) && (-e.e1 > e.D0)) w1 = 0.f;
+    if ((h1 < s.eps_h) && (-e.e0 > e.D1)) w0 = 0.f;
+    const float h0rg = inv_depth(h0, s.eps_h), h1rg = inv_depth(h1, s.eps_h);
+    float u0n = h0rg * w0, u1n = h1rg * w1;
+    w0 = u0n * h0;
+    w1 = u1n * h1;
+    const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+    float uijn = (s0 * u0n + s1 * u1n) / (s0 + s1 + kEps);
+    const float val = (2.f * ilcos * dt) / (e.area0 + e.area1);
+    const float c0 = sqrtf(hij);
+    const float aut1 = fmin_(uijn - c0, u0n - s0);
+    const float aut2 = fmax_(uijn + c0, u1n + s1);
+    float maxa = fmax_(fabsf(aut2), fabsf(aut1));
+    const float fl1x = w1, fl1y = u1n * w1, fl0x = w0, fl0y = u0n * w0;
+    const float dq = fl1x - fl0x;
+    const float deta = surface_jump(e.e0, e.e1, e.D0, e.D1);
+    float s_my, s_py, s_mz, s_pz;
+    if (uijn < 0.f) {
+        s_my = u1n * w1 * ilcos * e.normal; s_py = -s_my; s_my += hij * deta * ilcos;
+        s_mz = u1n * e.v1 * ilcos; s_pz = -s_mz;
+    } else {
+        s_my = u0n * w0 * ilcos * e.normal; s_py = -s_my; s_my += hij * deta * ilcos;
+        s_mz = u0n * e.v0 * ilcos; s_pz = -s_mz;
+    }
+    const float cd = 0.5f * (1.f - s.cvis / (1.f + __expf(-20.f * (1.f - s.hpos / hij))));
+    const float des = cd * val * maxa * maxa * dq * ilcos * e.normal;
+    s_my -= des;
+    s_py += des;
+    float xiL = 0.f, xiR = 0.f;
+    if (!e.no_lim) {
+        xiL = monotone_limiter(e.e0m, e.e0, e.e1, e.e1p, aut1);
+        xiR = monotone_limiter(e.e0m, e.e0, e.e1, e.e1p, aut2);
+    }
+    float a0, a1;
+    if (fabsf(aut1 - aut2) >= kEps) {
+        const float alr = sgnf(aut1) * (1.f - xiL) + val * aut1 * xiL;
+        const float blr = sgnf(aut2) * (1.f - xiR) + val * aut2 * xiR;
+        const float aux = 1.f / (aut2 - aut1);
+        a0 = (alr - blr) * (aut1 * aut2) * aux;
+        a1 = (blr * aut2 - alr * aut1) * aux;
+    } else {
+        a0 = maxa;
+        a1 = 0.f;
+    }
+    float mx = 0.5f * dq, px = mx;
+    float my = 0.5f * (fl1y - fl0y + hij * deta), py = my;
+    const float desx = 0.5f * a0 * deta, desy = 0.5f * a0 * dq + a1 * my;
+    mx += fl0x - desx; my += fl0y - desy;
+    px += desx - fl1x; py += desy - fl1y;
+    mx *= ilcos; my *= ilcos; px *= ilcos; py *= ilcos;
+    // transverse momentum carried with a limited tangential velocity
+    const float q0mt = e.v0m * e.normal, q0t = e.v0 * e.normal, q1t = e.v1 * e.normal, q1pt = e.v1p * e.normal;
+    const float p0m = inv_depth(e.h0m, s.eps_h) * q0mt;
+    const float p1p = inv_depth(e.h1p, s.eps_h) * q1pt;
+    u0n = h0rg * q0t;
+    u1n = h1rg * q1t;
+    const float sg = -1.f * (mx < 0.f) + 1.f * (mx > 0.f);
+    uijn = fabsf(uijn) * sg;
+    const float xit = e.no_lim ? 0.f : monotone_limiter(p0m, u0n, u1n, p1p, uijn);
+    const float uijt = 0.5f * (u0n + u1n) - 0.5f * ((1.f - xit) * sg + xit * uijn * val) * (u1n - u0n);
+    const float aux = mx * uijt;
+    const float t_py = py * e.normal, t_pz = -aux * e.normal, t_my = my * e.normal, t_mz = aux * e.normal;
+    const float alfa = blend_2s(hij, s.hpos, e.no_lim);
+    r.m_x = alfa * s_my + (1.f - alfa) * t_my;
+    r.m_y = alfa * s_mz + (1.f - alfa) * t_mz;
+    r.p_x = alfa * s_py + (1.f - alfa) * t_py;
+    r.p_y = alfa * s_pz + (1.f - alfa) * t_pz;
+    if (maxa < s.eps_h) maxa += s.eps_h;
+    r.lam = ilcos * maxa;
+    return r;
+}
+
+// ---------------------------------------------------------------------------
+// phase 2: momentum flux of a y edge (src/GPU/Arista_kernel.cu:780-1026).
+// Edge "u" is qy, "v" is qx; components returned as (qx, qy).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ MomFlux momentum_flux_y(Edge &e, const ScenarioDev &s, float dt)
+{
+    MomFlux r;
+    r.active = true;
+    const float len = e.len;
+    if (all_deep(e, s.hpos)) {
+        const float icos0 = __frcp_rn(e.cos0), icos1 = __frcp_rn(e.cos1);
+        const float h0 = e.h0, h1 = e.h1, hij = 0.5f * (h0 + h1);
+        const float u0n = __fdividef(e.u0, h0), u1n = __fdividef(e.u1, h1);
+        const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+        const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
+        const float maxa = fabsf(uijn) + sqrtf(hij);
+        const float deta = 0.5f * (e.cos0 + e.cos1) * surface_jump(e.e0, e.e1, e.D0, e.D1) -
+                           uijn * uijn * (e.cos1 - e.cos0);
+        float fym, fyp, fxm, fxp;
+        if (uijn < 0.f) {
+            fym = u1n * e.u1 * len; fyp = -fym; fym *= e.cos1 * icos0; fym += hij * deta * len * icos0;
+            fxm = u1n * e.v1 * len; fxp = -fxm;
+        } else {
+            fym = u0n * e.u0 * len; fyp = -fym * e.cos0 * icos1; fym += hij * deta * len * icos0;
+            fxm = u0n * e.v0 * len; fxp = -fxm;
+        }
+        const float val = (2.f * len * dt) / (e.area0 + e.area1);
+        const float cd = 0.5f * (1.f - s.cvis);
+        const float des = cd * val * maxa * maxa * (e.u1 * e.cos1 - e.u0 * e.cos0) * len;
+        r.m_x = fxm; r.m_y = fym - des * icos0;
+        r.p_x = fxp; r.p_y = fyp + des * icos1;
+        r.lam = len * maxa;
+        return r;
+    }
+    if (e.front) swap_sides(e);
+    const float h0 = e.h0, h1 = e.h1;
+    if (!((h0 > kEps) || (h1 > kEps))) { r.active = false; return r; }
+    const float icos0 = __frcp_rn(e.cos0), icos1 = __frcp_rn(e.cos1);
+    float w0 = e.u0 * e.normal, w1 = e.u1 * e.normal;
+    const float hij = 0.5f * (h0 + h1);
+    const float c0 = sqrtf(hij);
+    if ((h0 < s.eps_h) && (-e.e1 > e.D0)) w1 = 0.f;
+    if ((h1 < s.eps_h) && (-e.e0 > e.D1)) w0 = 0.f;
+    const float h0rg = inv_depth(h0, s.eps_h), h1rg = inv_depth(h1, s.eps_h);
+    float u0n = h0rg * w0, u1n = h1rg * w1;
+    const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+    float uijn = (s0 * u0n + s1 * u1n) / (s0 + s1 + kEps);
+    const float val = (2.f * len * dt) / (e.area0 + e.area1);
+    const float aut1 = fmin_(uijn - c0, u0n - s0);
+    const float aut2 = fmax_(uijn + c0, u1n + s1);
+    float maxa = fmax_(fabsf(aut2), fabsf(aut1));
+    const float deta = 0.5f * (e.cos0 + e.cos1) * surface_jump(e.e0, e.e1, e.D0, e.D1) - uijn * uijn * (e.cos1 - e.cos0);
+    float s_mz, s_pz, s_my, s_py;
+    if (uijn < 0.f) {
+        s_mz = u1n * w1 * len * e.normal; s_pz = -s_mz; s_mz *= e.cos1 * icos0; s_mz += hij * deta * len * icos0;
+        s_my = u1n * e.v1 * len; s_py = -s_my;
+    } else {
+        s_mz = u0n * w0 * len * e.normal; s_pz = -s_mz * e.cos0 * icos1; s_mz += hij * deta * len * icos0;
+        s_my = u0n * e.v0 * len; s_py = -s_my;
+    }
+    const float cd = 0.5f * (1.f - s.cvis / (1.f + __expf(-20.f * (1.f - s.hpos / hij))));
+    const float fl1x = w1 * e.cos1, fl1y = u1n * fl1x, fl0x = w0 * e.cos0, fl0y = u0n * fl0x;
+    const float dq = fl1x - fl0x;
+    const float des = cd * val * maxa * maxa * dq * len;
+    s_mz -= des * icos0;
+    s_pz += des * icos1;
+    float xiL = 0.f, xiR = 0.f;
+    if (!e.no_lim) {
+        xiL = monotone_limiter(e.e0m, e.e0, e.e1, e.e1p, aut1);
+        xiR = monotone_limiter(e.e0m, e.e0, e.e1, e.e1p, aut2);
+    }
+    float a0, a1;
+    if (fabsf(aut1 - aut2) >= kEps) {
+        const float alr = sgnf(aut1) * (1.f - xiL) + val * aut1 * xiL;
+        const float blr = sgnf(aut2) * (1.f - xiR) + val * aut2 * xiR;
+        const float aux = 1.f / (aut2 - aut1);
+        a0 = (alr - blr) * (aut1 * aut2) * aux;
+        a1 = (blr * aut2 - alr * aut1) * aux;
+    } else {
+        a0 = maxa;
+        a1 = 0.f;
+    }
+    float mx = 0.5f * dq, px = mx;
+    float my = 0.5f * (fl1y - fl0y + hij * deta), py = my;
+    const float desx = 0.5f * a0 * deta, desy = 0.5f * a0 * dq + a1 * my;
+    mx += fl0x - desx; my += fl0y - desy;
+    px += desx - fl1x; py += desy - fl1y;
+    mx *= len; my *= len; px *= len; py *= len;
+    const float q0mt = -e.v0m * e.normal, q0t = -e.v0 * e.normal, q1t = -e.v1 * e.normal, q1pt = -e.v1p * e.normal;
+    const float p0m = inv_depth(e.h0m, s.eps_h) * q0mt;
+    const float p1p = inv_depth(e.h1p, s.eps_h) * q1pt;
+    u0n = h0rg * q0t;
+    u1n = h1rg * q1t;
+    const float sg = -1.f * (mx < 0.f) + 1.f * (mx > 0.f);
+    uijn = fabsf(uijn) * sg;
+    const float xit = e.no_lim ? 0.f : monotone_limiter(p0m, u0n, u1n, p1p, uijn);
+    const float uijt = 0.5f * (u0n * icos0 + u1n * icos1) -
+                       0.5f * ((1.f - xit) * sg + xit * uijn * val) * (u1n * icos1 - u0n * icos0);
+    const float aux = mx * uijt;
+    const float t_py = aux * e.normal, t_pz = py * e.normal * icos1;
+    const float t_my = -aux * e.normal, t_mz = my * e.normal * icos0;
+    if (maxa < s.eps_h) maxa += s.eps_h;
+    const float alfa = blend_2s(hij, s.hpos, e.no_lim);
+    r.m_x = alfa * s_my + (1.f - alfa) * t_my;
+    r.m_y = alfa * s_mz + (1.f - alfa) * t_mz;
+    r.p_x = alfa * s_py + (1.f - alfa) * t_py;
+    r.p_y = alfa * s_pz + (1.f - alfa) * t_pz;
+    r.lam = len * maxa;
+    return r;
+}
+
+}  // namespace thy

@@ -1,0 +1,46 @@
+// Launch wrappers of the device kernels (host-callable, no CUDA types beyond
+// cudaStream_t / int2 in the signatures).
+#pragma once
+#include <cstddef>
+#include <cuda_runtime.h>
+
+namespace thy {
+
+struct ScenarioDev;
+
+constexpr int kTileX = 32;        // tile width (cells)
+constexpr int kTileY = 16;        // tile height (cells)
+constexpr int kStepThreads = 256;
+
+// step.cu
+size_t step_smem_bytes();
+cudaError_t configure_step_kernels();
+int step_blocks_per_sm();
+// phase 0: initial dt; 1: mass + diagnostics; 2: momentum + dt + controller
+void launch_step_phase(int phase, const ScenarioDev *scen, const int2 *work, const int *nwork, int grid, cudaStream_t st);
+
+// init.cu: double-precision host state (reference layout, dimensionless) to
+// the FP32 device state; metrics initialised as in src/GPU/ShallowWater.cu:305-309
+void launch_init_state(const ScenarioDev *s_host, const ScenarioDev *s_dev, const double *h, const double *Hs,
+                       const double *qx, const double *qy, double Hmin, cudaStream_t st);
+
+// okada.cu: FP64 Okada deformation of one fault into a double scratch field,
+// |U_Z| max (for relative cropping), crop and apply
+struct OkadaFault {
+    double lon_c, lat_c, depth_c, length, width, strike, dip, rake, slip;
+};
+void launch_okada(const ScenarioDev *s_host, double *def, double lon0, double dlon, double lat0, double dlat,
+                  const OkadaFault &f, double Hs, cudaStream_t st);
+void launch_absmax(const double *def, long long n, unsigned int *max_bits, cudaStream_t st);
+void launch_apply_deformation(const ScenarioDev *s_host, const double *def, int crop_flag, double crop_value,
+                              const unsigned int *max_bits, cudaStream_t st);
+
+// extract.cu: dimensional output fields (src/GPU/netcdf_kernel.cu)
+enum Field { kFieldEta = 0, kFieldUx = 1, kFieldUy = 2, kFieldMaxHeight = 3, kFieldArrival = 4, kFieldDeformed = 5 };
+void launch_extract(const ScenarioDev *s_host, int field, int parity, float *out, double Hs, double Qs, double Hmin,
+                    cudaStream_t st);
+// gauges: eta (m), ux, uy (m/s) and depth at nP cells (cell index or -1)
+void launch_gauges(const ScenarioDev *s_host, int parity, const int *cells, int nP, float *out4, double Hs, double Qs,
+                   double Hmin, cudaStream_t st);
+
+}  // namespace thy

@@ -13,7 +13,10 @@
  * and so that common readers (e.g. scipy.io.netcdf_file) open them.
  */
 #define _FILE_OFFSET_BITS 64
+#define _POSIX_C_SOURCE 200809L
 #include "netcdf.h"
+
+#include <sys/types.h>
 
 #include <stdint.h>
 #include <stdio.h>

@@ -1,0 +1,679 @@
+// Host engine of the B200 stepper: device state of a scenario, the batch
+// (work list + CUDA graph of stepping kernels), the event-driven time loop
+// of src/GPU/ShallowWater.cu:396-450 and the C ABI entry points thy_run /
+// thy_session_* / thy_device_*.
+//
+// The time loop stays on the device: dt, the simulated time and the event
+// checks live in a per-scenario control block updated by the last tile of
+// each phase-2 launch, so steps are launched in graph chunks with one host
+// synchronisation per chunk instead of one blocking copy per step.  When an
+// event is due (fault time, snapshot time, gauge time) the controller pauses
+// the scenario; later launches of the chunk do nothing for it, and the host
+// performs the event exactly at that step before resuming.
+#include "engine.h"
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+
+namespace thy {
+
+namespace {
+thread_local char g_err[512] = "";
+int g_device = 0;
+bool g_configured[64] = {};
+int g_sms[64] = {};
+}  // namespace
+
+void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line)
+{
+    snprintf(g_err, sizeof(g_err), "%s (%s) at %s:%d", cudaGetErrorString(e), what, file, line);
+}
+
+const char *last_error_text() { return g_err; }
+
+int ensure_device()
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return THY_ERR_NO_DEVICE;
+    }
+    if (g_device >= n) return THY_ERR_INVALID;
+    THY_CK(cudaSetDevice(g_device));
+    if (!g_configured[g_device]) {
+        THY_CK(configure_step_kernels());
+        THY_CK(cudaDeviceGetAttribute(&g_sms[g_device], cudaDevAttrMultiProcessorCount, g_device));
+        g_configured[g_device] = true;
+    }
+    return THY_OK;
+}
+
+int device_sm_count() { return g_sms[g_device] > 0 ? g_sms[g_device] : 148; }
+
+static int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+size_t scenario_bytes(int nx, int ny, bool has_faults)
+{
+    const size_t pitch = (size_t)round_up(nx, 32);
+    size_t b = 10 * pitch * ny * sizeof(float);          // fields
+    b += (size_t)(5 * ny + 1) * sizeof(float);           // row tables
+    b += 3 * (size_t)nx * ny * sizeof(float);            // output staging
+    if (has_faults) b += (size_t)nx * ny * sizeof(double);
+    return b + 4096;
+}
+
+// ---------------------------------------------------------------------------
+// DevScenario
+// ---------------------------------------------------------------------------
+
+DevScenario::~DevScenario()
+{
+    cudaFree(fields);
+    cudaFree(rows);
+    cudaFree(def);
+    cudaFree(maxbits);
+    cudaFree(d_cells);
+    cudaFree(d_gauge);
+    cudaFree(d_out);
+    cudaFree(fault_times_d);
+}
+
+int DevScenario::setup(const thy_problem *p, cudaStream_t st)
+{
+    if (!p || p->nx < 2 || p->ny < 2 || !p->h || !p->Hs || !p->area_cos || !p->dlon || !p->dlat || !p->lon || !p->lat)
+        return THY_ERR_INVALID;
+    nx = p->nx;
+    ny = p->ny;
+    pitch = round_up(nx, 32);
+    plane = (size_t)pitch * ny;
+    const size_t n = (size_t)nx * ny;
+    Hs = p->H;
+    Qs = p->Q;
+    Ts = p->T;
+    Ls = p->L;
+    Hmin = p->Hmin;
+    t_end = p->t_end;
+    save_nc = p->save_nc;
+    save_ts = (p->npoints > 0) ? p->save_ts : -1.0;
+    max_steps = p->max_steps;
+    crop_flag = p->crop_flag;
+    crop_value = p->crop_value;
+    okada_flag = p->okada_flag;
+    lon0 = p->lon[0];
+    lat0 = p->lat[0];
+    dlon = (p->lon[nx - 1] - p->lon[0]) / (nx - 1);
+    dlat = (p->lat[ny - 1] - p->lat[0]) / (ny - 1);
+    faults.assign(p->faults ? p->faults : (const double *)nullptr,
+                  p->faults ? p->faults + 10 * (size_t)std::max(p->nfaults, 0) : nullptr);
+    cells.assign(p->point_cell ? p->point_cell : (const int *)nullptr,
+                 p->point_cell ? p->point_cell + std::max(p->npoints, 0) : nullptr);
+    const int nf = (int)(faults.size() / 10);
+
+    THY_CK(cudaMalloc(&fields, 10 * plane * sizeof(float)));
+    THY_CK(cudaMalloc(&rows, (size_t)(5 * ny + 1) * sizeof(float)));
+    THY_CK(cudaMalloc(&d_out, 3 * n * sizeof(float)));
+    if (nf > 0) {
+        THY_CK(cudaMalloc(&def, n * sizeof(double)));
+        THY_CK(cudaMalloc(&maxbits, sizeof(unsigned int)));
+        THY_CK(cudaMalloc(&fault_times_d, nf * sizeof(double)));
+        std::vector<double> tf(nf);
+        for (int i = 0; i < nf; i++) tf[i] = faults[10 * i];
+        THY_CK(cudaMemcpyAsync(fault_times_d, tf.data(), nf * sizeof(double), cudaMemcpyHostToDevice, st));
+        THY_CK(cudaStreamSynchronize(st));
+    }
+    if (!cells.empty()) {
+        THY_CK(cudaMalloc(&d_cells, cells.size() * sizeof(int)));
+        THY_CK(cudaMalloc(&d_gauge, 4 * cells.size() * sizeof(float)));
+        THY_CK(cudaMemcpyAsync(d_cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+        ts_min.assign(cells.size(), 1e30f);
+        ts_max.assign(cells.size(), -1e30f);
+        for (size_t i = 0; i < cells.size(); i++)
+            if (cells[i] < 0) ts_min[i] = ts_max[i] = -9999.0f;
+    }
+
+    // per-row metric terms: computed in FP64, stored once as FP32
+    {
+        std::vector<float> r((size_t)(5 * ny + 1));
+        float *cosr = r.data(), *ilc = cosr + ny, *ar = ilc + ny, *dlo = ar + ny, *dla = dlo + ny + 1;
+        for (int y = 0; y < ny; y++) {
+            const double area = p->area_cos[2 * y], c = p->area_cos[2 * y + 1];
+            cosr[y] = (float)c;
+            ilc[y] = (float)(p->dlat[y] / c);
+            ar[y] = (float)area;
+            dla[y] = (float)p->dlat[y];
+        }
+        for (int y = 0; y <= ny; y++) dlo[y] = (float)p->dlon[y];
+        THY_CK(cudaMemcpyAsync(rows, r.data(), r.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        THY_CK(cudaStreamSynchronize(st));
+        desc.row.cosphi = rows;
+        desc.row.ilcos = rows + ny;
+        desc.row.area = rows + 2 * ny;
+        desc.row.dlon = rows + 3 * ny;
+        desc.row.dlat = rows + 4 * ny + 1;
+    }
+
+    desc.nx = nx;
+    desc.ny = ny;
+    desc.pitch = pitch;
+    desc.tiles_x = (nx + kTileX - 1) / kTileX;
+    desc.tiles_y = (ny + kTileY - 1) / kTileY;
+    desc.ntiles = desc.tiles_x * desc.tiles_y;
+    desc.periodic = (std::fabs(p->border_left - 2.0) < 2.220446049250313e-16) &&
+                    (std::fabs(p->border_right - 2.0) < 2.220446049250313e-16);
+    desc.b_up = (float)p->border_up;
+    desc.b_low = (float)p->border_low;
+    desc.b_left = (float)p->border_left;
+    desc.b_right = (float)p->border_right;
+    desc.sp_up = p->sponge_up;
+    desc.sp_low = p->sponge_low;
+    desc.sp_left = p->sponge_left;
+    desc.sp_right = p->sponge_right;
+    desc.cfl = (float)p->cfl;
+    desc.eps_h = (float)p->eps_h;
+    desc.eps_h64 = p->eps_h;
+    desc.hpos = (float)p->hpos;
+    desc.cvis = (float)p->cvis;
+    desc.mf0 = (float)p->mf0;
+    desc.vmax = (float)p->vmax;
+    desc.dif_at = (float)p->dif_at;
+    desc.sea = 0.f;
+    for (int k = 0; k < 2; k++) {
+        desc.eta[k] = fields + (0 + k) * plane;
+        desc.qx[k] = fields + (2 + k) * plane;
+        desc.qy[k] = fields + (4 + k) * plane;
+    }
+    desc.dep = fields + 6 * plane;
+    desc.eta_max = fields + 7 * plane;
+    desc.arr = fields + 8 * plane;
+    desc.eta_ini = fields + 9 * plane;
+
+    // dimensionless double state -> FP32 device state
+    {
+        double *tmp = nullptr;
+        const bool hasq = p->qx && p->qy;
+        THY_CK(cudaMalloc(&tmp, (hasq ? 4 : 2) * n * sizeof(double)));
+        THY_CK(cudaMemcpyAsync(tmp, p->h, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        THY_CK(cudaMemcpyAsync(tmp + n, p->Hs, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        if (hasq) {
+            THY_CK(cudaMemcpyAsync(tmp + 2 * n, p->qx, n * sizeof(double), cudaMemcpyHostToDevice, st));
+            THY_CK(cudaMemcpyAsync(tmp + 3 * n, p->qy, n * sizeof(double), cudaMemcpyHostToDevice, st));
+        }
+        launch_init_state(&desc, nullptr, tmp, tmp + n, hasq ? tmp + 2 * n : nullptr, hasq ? tmp + 3 * n : nullptr, Hmin, st);
+        THY_CK(cudaGetLastError());
+        THY_CK(cudaStreamSynchronize(st));
+        cudaFree(tmp);
+    }
+
+    std::memset(&hctl, 0, sizeof(hctl));
+    hctl.t = 0.0;
+    hctl.dt = 0.0;
+    hctl.t_end = t_end;
+    hctl.save_nc = save_nc;
+    hctl.next_nc = 0.0;
+    hctl.save_ts = save_ts;
+    hctl.next_ts = 0.0;
+    hctl.T = Ts;
+    hctl.step = 0;
+    hctl.max_steps = max_steps;
+    hctl.status = kRunning;
+    hctl.parity = 0;
+    hctl.fault_next = 0;
+    hctl.jumping = 0;
+    hctl.nfaults = nf;
+    hctl.fault_times = fault_times_d;
+    hctl.dt_bits = 0x7f7fffffu;
+    hctl.tiles_done = 0;
+    hctl.errors = 0;
+    return THY_OK;
+}
+
+int DevScenario::upload_ctl(cudaStream_t st)
+{
+    THY_CK(cudaMemcpyAsync(ctl, &hctl, sizeof(ScenarioCtl), cudaMemcpyHostToDevice, st));
+    return THY_OK;
+}
+
+int DevScenario::download_ctl(cudaStream_t st)
+{
+    THY_CK(cudaMemcpyAsync(&hctl, ctl, sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, st));
+    return THY_OK;
+}
+
+// src/GPU/ShallowWater.cu:125-147: every fault whose time has been reached
+int DevScenario::apply_due_faults(cudaStream_t st)
+{
+    const int nf = (int)(faults.size() / 10);
+    while (hctl.fault_next < nf && hctl.t * Ts >= faults[10 * hctl.fault_next]) {
+        const double *f = &faults[10 * hctl.fault_next];
+        OkadaFault of{f[1], f[2], f[3], f[4], f[5], f[6], f[7], f[8], f[9]};
+        launch_okada(&desc, def, lon0, dlon, lat0, dlat, of, Hs, st);
+        if (crop_flag == 1) launch_absmax(def, (long long)nx * ny, maxbits, st);
+        // the apply kernel reads the parity from the control block
+        THY_CK(cudaMemcpyAsync(ctl, &hctl, sizeof(ScenarioCtl), cudaMemcpyHostToDevice, st));
+        launch_apply_deformation(&desc, def, crop_flag, crop_value, maxbits, st);
+        THY_CK(cudaGetLastError());
+        hctl.fault_next++;
+    }
+    return THY_OK;
+}
+
+int DevScenario::extract(int field, float *host_out, cudaStream_t st)
+{
+    const size_t n = (size_t)nx * ny;
+    launch_extract(&desc, field, hctl.parity, d_out, Hs, Qs, Hmin, st);
+    THY_CK(cudaGetLastError());
+    THY_CK(cudaMemcpyAsync(host_out, d_out, n * sizeof(float), cudaMemcpyDeviceToHost, st));
+    THY_CK(cudaStreamSynchronize(st));
+    return THY_OK;
+}
+
+int DevScenario::snapshot(const thy_outputs *o, cudaStream_t st)
+{
+    const size_t n = (size_t)nx * ny;
+    if (o && o->on_snapshot) {
+        std::vector<float> buf(3 * n);
+        for (int k = 0; k < 3; k++) {
+            launch_extract(&desc, kFieldEta + k, hctl.parity, d_out + k * n, Hs, Qs, Hmin, st);
+        }
+        THY_CK(cudaGetLastError());
+        THY_CK(cudaMemcpyAsync(buf.data(), d_out, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st));
+        THY_CK(cudaStreamSynchronize(st));
+        o->on_snapshot(o->user, snapshots, hctl.t * Ts, buf.data(), buf.data() + n, buf.data() + 2 * n);
+    }
+    snapshots++;
+    return THY_OK;
+}
+
+int DevScenario::sample_gauges(const thy_outputs *o, cudaStream_t st)
+{
+    const int np = (int)cells.size();
+    if (np > 0) {
+        std::vector<float> g(4 * (size_t)np), e(np), ux(np), uy(np);
+        launch_gauges(&desc, hctl.parity, d_cells, np, d_gauge, Hs, Qs, Hmin, st);
+        THY_CK(cudaGetLastError());
+        THY_CK(cudaMemcpyAsync(g.data(), d_gauge, g.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        THY_CK(cudaStreamSynchronize(st));
+        for (int i = 0; i < np; i++) {
+            e[i] = g[4 * i];
+            ux[i] = g[4 * i + 1];
+            uy[i] = g[4 * i + 2];
+            if (cells[i] >= 0) {
+                ts_min[i] = (ts_min[i] < e[i]) ? ts_min[i] : e[i];
+                ts_max[i] = (e[i] < ts_max[i]) ? ts_max[i] : e[i];
+            }
+        }
+        if (o && o->on_series) o->on_series(o->user, series, hctl.t * Ts, e.data(), ux.data(), uy.data());
+    }
+    series++;
+    return THY_OK;
+}
+
+int DevScenario::finish(const thy_outputs *o, cudaStream_t st)
+{
+    if (!o) return THY_OK;
+    int rc;
+    if (o->max_height && (rc = extract(kFieldMaxHeight, o->max_height, st))) return rc;
+    if (o->arrival && (rc = extract(kFieldArrival, o->arrival, st))) return rc;
+    if (o->deformed_bathy && (rc = extract(kFieldDeformed, o->deformed_bathy, st))) return rc;
+    if (o->eta && (rc = extract(kFieldEta, o->eta, st))) return rc;
+    if (o->ux && (rc = extract(kFieldUx, o->ux, st))) return rc;
+    if (o->uy && (rc = extract(kFieldUy, o->uy, st))) return rc;
+    const int np = (int)cells.size();
+    if (np > 0 && (o->series_min || o->series_max || o->series_bathy)) {
+        std::vector<float> g(4 * (size_t)np);
+        launch_gauges(&desc, hctl.parity, d_cells, np, d_gauge, Hs, Qs, Hmin, st);
+        THY_CK(cudaGetLastError());
+        THY_CK(cudaMemcpyAsync(g.data(), d_gauge, g.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        THY_CK(cudaStreamSynchronize(st));
+        for (int i = 0; i < np; i++) {
+            if (o->series_min) o->series_min[i] = ts_min[i];
+            if (o->series_max) o->series_max[i] = ts_max[i];
+            if (o->series_bathy) o->series_bathy[i] = g[4 * i + 3];
+        }
+    }
+    return THY_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Batch
+// ---------------------------------------------------------------------------
+
+Batch::~Batch()
+{
+    if (gexec) cudaGraphExecDestroy(gexec);
+    cudaFree(d_table);
+    cudaFree(d_work);
+    cudaFree(d_nwork);
+    cudaFree(d_ctl);
+    cudaFreeHost(h_ctl);
+    if (ev0) cudaEventDestroy(ev0);
+    if (ev1) cudaEventDestroy(ev1);
+}
+
+int Batch::init(int cap, int max_work, cudaStream_t stream)
+{
+    capacity = cap;
+    work_capacity = max_work;
+    st = stream;
+    THY_CK(cudaMalloc(&d_table, cap * sizeof(ScenarioDev)));
+    THY_CK(cudaMalloc(&d_ctl, cap * sizeof(ScenarioCtl)));
+    THY_CK(cudaMallocHost(&h_ctl, cap * sizeof(ScenarioCtl)));
+    THY_CK(cudaMalloc(&d_work, std::max(max_work, 1) * sizeof(int2)));
+    THY_CK(cudaMalloc(&d_nwork, sizeof(int)));
+    THY_CK(cudaEventCreate(&ev0));
+    THY_CK(cudaEventCreate(&ev1));
+    std::vector<ScenarioCtl> z(cap);
+    for (auto &c : z) { std::memset(&c, 0, sizeof(c)); c.status = kIdle; }
+    THY_CK(cudaMemcpyAsync(d_ctl, z.data(), cap * sizeof(ScenarioCtl), cudaMemcpyHostToDevice, st));
+    THY_CK(cudaStreamSynchronize(st));
+    members.assign(cap, nullptr);
+    return THY_OK;
+}
+
+int Batch::attach(DevScenario *s)
+{
+    for (int i = 0; i < capacity; i++) {
+        if (!members[i]) {
+            members[i] = s;
+            s->ctl = d_ctl + i;
+            s->desc.ctl = s->ctl;
+            return THY_OK;
+        }
+    }
+    return THY_ERR_BUDGET;
+}
+
+int Batch::detach(DevScenario *s)
+{
+    for (int i = 0; i < capacity; i++)
+        if (members[i] == s) {
+            members[i] = nullptr;
+            ScenarioCtl z;
+            std::memset(&z, 0, sizeof(z));
+            z.status = kIdle;
+            THY_CK(cudaMemcpyAsync(d_ctl + i, &z, sizeof(z), cudaMemcpyHostToDevice, st));
+            s->ctl = nullptr;
+        }
+    return THY_OK;
+}
+
+int Batch::rebuild()
+{
+    std::vector<ScenarioDev> table(capacity);
+    std::vector<int2> work;
+    for (int i = 0; i < capacity; i++) {
+        if (!members[i]) continue;
+        table[i] = members[i]->desc;
+        for (int t = 0; t < members[i]->desc.ntiles; t++) work.push_back(make_int2(i, t));
+    }
+    if ((int)work.size() > work_capacity) {
+        cudaFree(d_work);
+        work_capacity = (int)work.size();
+        THY_CK(cudaMalloc(&d_work, work_capacity * sizeof(int2)));
+    }
+    nwork = (int)work.size();
+    THY_CK(cudaMemcpyAsync(d_table, table.data(), capacity * sizeof(ScenarioDev), cudaMemcpyHostToDevice, st));
+    if (nwork) THY_CK(cudaMemcpyAsync(d_work, work.data(), nwork * sizeof(int2), cudaMemcpyHostToDevice, st));
+    THY_CK(cudaMemcpyAsync(d_nwork, &nwork, sizeof(int), cudaMemcpyHostToDevice, st));
+    THY_CK(cudaStreamSynchronize(st));
+    const int bps = std::max(1, step_blocks_per_sm());
+    grid = std::max(1, std::min(nwork, device_sm_count() * bps * 8));
+    if (gexec) {
+        cudaGraphExecDestroy(gexec);
+        gexec = nullptr;
+    }
+    cudaGraph_t g;
+    THY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int k = 0; k < chunk; k++) {
+        launch_step_phase(1, d_table, d_work, d_nwork, grid, st);
+        launch_step_phase(2, d_table, d_work, d_nwork, grid, st);
+    }
+    THY_CK(cudaStreamEndCapture(st, &g));
+    cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+    cudaGraphDestroy(g);
+    THY_CK(e);
+    return THY_OK;
+}
+
+int Batch::run_chunk(bool timed)
+{
+    if (timed) THY_CK(cudaEventRecord(ev0, st));
+    THY_CK(cudaGraphLaunch(gexec, st));
+    if (timed) THY_CK(cudaEventRecord(ev1, st));
+    THY_CK(cudaMemcpyAsync(h_ctl, d_ctl, capacity * sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, st));
+    THY_CK(cudaStreamSynchronize(st));
+    if (timed) {
+        float ms = 0;
+        THY_CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        device_ms += ms;
+    }
+    launches += 2LL * chunk;
+    for (int i = 0; i < capacity; i++)
+        if (members[i]) members[i]->hctl = h_ctl[i];
+    return THY_OK;
+}
+
+// Initial dt of every member (src/GPU/Timestep.cu:11-33) and the truncation
+// to the first fault time (src/GPU/ShallowWater.cu:382-391).
+static int initial_dt(Batch &b)
+{
+    int rc;
+    for (auto *s : b.members)
+        if (s && (rc = s->upload_ctl(b.st))) return rc;
+    launch_step_phase(0, b.d_table, b.d_work, b.d_nwork, b.grid, b.st);
+    THY_CK(cudaGetLastError());
+    THY_CK(cudaMemcpyAsync(b.h_ctl, b.d_ctl, b.capacity * sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, b.st));
+    THY_CK(cudaStreamSynchronize(b.st));
+    for (int i = 0; i < b.capacity; i++) {
+        DevScenario *s = b.members[i];
+        if (!s) continue;
+        s->hctl = b.h_ctl[i];
+        double dt = s->hctl.dt, t = s->hctl.t, T = s->Ts;
+        const int nf = (int)(s->faults.size() / 10);
+        int jumping = 0;
+        if (nf > 0) {
+            const double *tf0 = &s->faults[0];
+            if (tf0[0] < 2.220446049250313e-16) {
+                int k = 1;
+                while (k < nf && !(std::fabs(s->faults[10 * k] - tf0[0]) > 2.220446049250313e-16)) k++;
+                if (k < nf && (t + dt) * T > s->faults[10 * k]) { dt = s->faults[10 * k] / T - t; jumping = 1; }
+            } else if ((t + dt) * T > tf0[0]) {
+                dt = tf0[0] / T - t;
+                jumping = 1;
+            }
+        }
+        s->hctl.dt = dt;
+        s->hctl.jumping = jumping;
+        s->first_dt_s = dt * T;
+    }
+    return THY_OK;
+}
+
+// Host side of one loop iteration's events (src/GPU/ShallowWater.cu:398-421).
+static int handle_events(DevScenario &s, const thy_outputs *o, cudaStream_t st)
+{
+    int rc;
+    if ((rc = s.apply_due_faults(st))) return rc;
+    if (s.save_nc >= 0.0 && s.hctl.t >= s.hctl.next_nc) {
+        s.hctl.next_nc += s.save_nc;
+        if ((rc = s.snapshot(o, st))) return rc;
+    }
+    if (s.save_ts >= 0.0 && s.hctl.t >= s.hctl.next_ts) {
+        s.hctl.next_ts += s.save_ts;
+        if ((rc = s.sample_gauges(o, st))) return rc;
+    }
+    return THY_OK;
+}
+
+}  // namespace thy
+
+using namespace thy;
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+
+extern "C" const char *thy_version(void) { return "thysea-b200 1.0 (Tsunami-HySEA 1.3.0 scheme)"; }
+
+extern "C" const char *thy_strerror(int code)
+{
+    switch (code) {
+    case THY_OK: return "ok";
+    case THY_ERR_GPU_MEMORY: return "not enough GPU memory";
+    case THY_ERR_HOST: return "host memory or output file error";
+    case THY_ERR_INVALID: return "invalid argument";
+    case THY_ERR_CUDA: return last_error_text()[0] ? last_error_text() : "CUDA error";
+    case THY_ERR_NO_DEVICE: return "there is no CUDA device";
+    case THY_ERR_NONFINITE: return "the state or the time step became non-finite";
+    case THY_ERR_BUDGET: return "scenario does not fit the HBM budget";
+    case THY_ERR_CANCELLED: return "request cancelled";
+    default: return "unknown error";
+    }
+}
+
+extern "C" int thy_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+extern "C" int thy_set_device(int device)
+{
+    if (device < 0 || device >= 64) return THY_ERR_INVALID;
+    g_device = device;
+    return THY_OK;
+}
+
+extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *stats)
+{
+    int rc = ensure_device();
+    if (rc) return rc;
+    if (!p) return THY_ERR_INVALID;
+    cudaStream_t st;
+    THY_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    auto t0 = std::chrono::steady_clock::now();
+    {
+        DevScenario s;
+        Batch b;
+        if ((rc = b.init(1, (p->nx / kTileX + 2) * (p->ny / kTileY + 2), st))) goto out;
+        if ((rc = b.attach(&s))) goto out;
+        if ((rc = s.setup(p, st))) goto out;
+        s.desc.ctl = s.ctl;
+        if ((rc = b.rebuild())) goto out;
+        t0 = std::chrono::steady_clock::now();
+        if ((rc = initial_dt(b))) goto out;
+        for (;;) {
+            if (!(s.hctl.t < s.t_end)) break;
+            if (s.max_steps >= 0 && s.hctl.step >= s.max_steps) break;
+            if (s.hctl.status == kFailed) { rc = THY_ERR_NONFINITE; goto out; }
+            if ((rc = handle_events(s, o, st))) goto out;
+            s.hctl.status = kRunning;
+            s.hctl.events = 0;
+            if ((rc = s.upload_ctl(st))) goto out;
+            do {
+                if ((rc = b.run_chunk(true))) goto out;
+            } while (s.hctl.status == kRunning);
+            if (s.hctl.status == kFailed) { rc = THY_ERR_NONFINITE; goto out; }
+        }
+        {
+            auto t1 = std::chrono::steady_clock::now();
+            if (stats) {
+                stats->steps = s.hctl.step;
+                stats->final_time_s = s.hctl.t * s.Ts;
+                stats->first_dt_s = s.first_dt_s;
+                stats->loop_seconds = std::chrono::duration<double>(t1 - t0).count();
+                stats->device_loop_ms = b.device_ms;
+                stats->kernel_launches = b.launches;
+                stats->snapshots = s.snapshots;
+                stats->series_samples = s.series;
+            }
+        }
+        rc = s.finish(o, st);
+    out:;
+    }
+    cudaStreamDestroy(st);
+    return rc;
+}
+
+// ---------------------------------------------------------------------------
+// sessions: step-level access for benchmarking
+// ---------------------------------------------------------------------------
+
+struct thy_session {
+    cudaStream_t st = nullptr;
+    DevScenario s;
+    Batch b;
+};
+
+extern "C" int thy_session_open(const thy_problem *p, thy_session **out)
+{
+    int rc = ensure_device();
+    if (rc) return rc;
+    if (!p || !out) return THY_ERR_INVALID;
+    thy_session *S = new thy_session();
+    THY_CK(cudaStreamCreateWithFlags(&S->st, cudaStreamNonBlocking));
+    thy_problem q = *p;
+    q.save_nc = -1.0;
+    q.save_ts = -1.0;
+    q.max_steps = 0;
+    if ((rc = S->b.init(1, (p->nx / kTileX + 2) * (p->ny / kTileY + 2), S->st)) || (rc = S->b.attach(&S->s)) ||
+        (rc = S->s.setup(&q, S->st)) || (rc = S->b.rebuild()) || (rc = initial_dt(S->b)) ||
+        (rc = S->s.apply_due_faults(S->st))) {
+        cudaStream_t st = S->st;
+        delete S;
+        cudaStreamDestroy(st);
+        return rc;
+    }
+    *out = S;
+    return THY_OK;
+}
+
+extern "C" int thy_session_steps(thy_session *S, long long steps, double *device_ms, long long *steps_done)
+{
+    if (!S) return THY_ERR_INVALID;
+    DevScenario &s = S->s;
+    const long long start = s.hctl.step;
+    const double ms0 = S->b.device_ms;
+    int rc;
+    s.hctl.max_steps = start + steps;
+    if (s.hctl.t < s.t_end && steps > 0) {
+        s.hctl.status = kRunning;
+        s.hctl.events = 0;
+        if ((rc = s.upload_ctl(S->st))) return rc;
+        do {
+            if ((rc = S->b.run_chunk(true))) return rc;
+        } while (s.hctl.status == kRunning);
+    }
+    if (device_ms) *device_ms = S->b.device_ms - ms0;
+    if (steps_done) *steps_done = s.hctl.step - start;
+    return s.hctl.status == kFailed ? THY_ERR_NONFINITE : THY_OK;
+}
+
+extern "C" int thy_session_fetch(thy_session *S, float *max_height, float *eta, float *ux, float *uy)
+{
+    if (!S) return THY_ERR_INVALID;
+    thy_outputs o;
+    std::memset(&o, 0, sizeof(o));
+    o.max_height = max_height;
+    o.eta = eta;
+    o.ux = ux;
+    o.uy = uy;
+    return S->s.finish(&o, S->st);
+}
+
+extern "C" double thy_session_time(const thy_session *S) { return S ? S->s.hctl.t * S->s.Ts : 0.0; }
+
+extern "C" void thy_session_close(thy_session *S)
+{
+    if (!S) return;
+    cudaStream_t st = S->st;
+    delete S;
+    if (st) cudaStreamDestroy(st);
+}

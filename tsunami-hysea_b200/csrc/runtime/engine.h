@@ -1,0 +1,108 @@
+// Host-side engine: device state of scenarios, the graph-captured time loop
+// and its event handling.  Shared by thy_run (one scenario), the session
+// API (benchmarking) and the batch / server runtimes (many scenarios in one
+// persistent launch).
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../../include/thysea.h"
+#include "../kernels/device.cuh"
+#include "../kernels/kernels.h"
+
+namespace thy {
+
+#define THY_CK(expr)                                                          \
+    do {                                                                      \
+        cudaError_t _e = (expr);                                              \
+        if (_e != cudaSuccess) {                                              \
+            set_last_cuda_error(_e, #expr, __FILE__, __LINE__);               \
+            return (_e == cudaErrorMemoryAllocation) ? THY_ERR_GPU_MEMORY : THY_ERR_CUDA; \
+        }                                                                     \
+    } while (0)
+
+void set_last_cuda_error(cudaError_t e, const char *what, const char *file, int line);
+const char *last_error_text();
+
+// Device bytes one scenario of nx*ny cells needs (fields, row tables, control,
+// Okada scratch when it has faults).
+size_t scenario_bytes(int nx, int ny, bool has_faults);
+
+// One scenario on the device.
+struct DevScenario {
+    int nx = 0, ny = 0, pitch = 0;
+    size_t plane = 0;              // floats per field plane
+    float *fields = nullptr;       // 10 planes: eta0 eta1 qx0 qx1 qy0 qy1 dep emax arr eini
+    float *rows = nullptr;         // row tables
+    double *def = nullptr;         // Okada scratch (nx*ny doubles)
+    unsigned int *maxbits = nullptr;
+    int *d_cells = nullptr;        // gauge cells
+    float *d_gauge = nullptr;      // 4 floats per gauge
+    float *d_out = nullptr;        // 3 planes nx*ny for snapshots / outputs
+    double *fault_times_d = nullptr;
+    ScenarioCtl *ctl = nullptr;    // device control block (owned by the batch slot)
+    ScenarioDev desc{};            // descriptor (device pointers), host copy
+    // problem data kept on the host
+    double Hs = 1, Qs = 1, Ts = 1, Hmin = 0, Ls = 1;
+    double lon0 = 0, dlon = 0, lat0 = 0, dlat = 0;
+    double t_end = 0, save_nc = -1, save_ts = -1;
+    long long max_steps = -1;
+    int crop_flag = 0;
+    double crop_value = 0;
+    std::vector<double> faults;    // 10 per fault, sorted by time
+    std::vector<int> cells;        // gauge cells
+    int okada_flag = 0;
+    // host mirror of the control block
+    ScenarioCtl hctl{};
+    // run bookkeeping
+    int snapshots = 0, series = 0;
+    std::vector<float> ts_min, ts_max;
+    double first_dt_s = 0;
+
+    ~DevScenario();
+    int setup(const thy_problem *p, cudaStream_t st);   // allocate, upload, initial dt
+    int upload_ctl(cudaStream_t st);
+    int download_ctl(cudaStream_t st);                   // async into hctl (pinned by the batch)
+    int apply_due_faults(cudaStream_t st);               // faults with time <= t (the loop's first action)
+    int extract(int field, float *host_out, cudaStream_t st);
+    int snapshot(const thy_outputs *o, cudaStream_t st);
+    int sample_gauges(const thy_outputs *o, cudaStream_t st);
+    int finish(const thy_outputs *o, cudaStream_t st);
+};
+
+// A set of scenarios stepped together: one work list over all their tiles,
+// one CUDA graph of `chunk` steps (2 launches per step).
+struct Batch {
+    std::vector<DevScenario *> members;
+    ScenarioDev *d_table = nullptr;
+    int2 *d_work = nullptr;
+    int *d_nwork = nullptr;
+    ScenarioCtl *d_ctl = nullptr;      // slots
+    ScenarioCtl *h_ctl = nullptr;      // pinned mirror
+    int capacity = 0;
+    int work_capacity = 0;
+    int nwork = 0;
+    int grid = 0;
+    int chunk = 16;
+    cudaStream_t st = nullptr;
+    cudaGraphExec_t gexec = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    double device_ms = 0;
+    long long launches = 0;
+
+    ~Batch();
+    int init(int capacity, int max_work, cudaStream_t stream);
+    int attach(DevScenario *s);      // gives s a control slot
+    int detach(DevScenario *s);
+    int rebuild();                    // tables + work list of RUNNING members; recapture the graph
+    int run_chunk(bool timed);       // one graph launch + control download (synchronous)
+};
+
+int ensure_device();
+int device_sm_count();
+
+}  // namespace thy

@@ -1,0 +1,189 @@
+"""thysea — Python host layer over libthysea.so, the B200 Tsunami-HySEA
+time stepper.
+
+The product is the C ABI in include/thysea.h; this module only marshals
+numpy arrays into it (ctypes), the way a Python caller of the reference
+would drive its shallowWater() through a small FFI stub.
+
+    from thysea import synth, run
+    p = synth.plain_small()
+    out = run(p)                      # max_height, arrival, eta, ... (numpy)
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import _ffi, synth  # noqa: F401
+
+THY_OK = 0
+
+
+class ThyError(RuntimeError):
+    def __init__(self, code: int, what: str):
+        self.code = code
+        msg = _ffi.lib().thy_strerror(code)
+        super().__init__(f"{what} failed: {code} ({msg.decode() if msg else ''})")
+
+
+def _check(code: int, what: str) -> None:
+    if code != THY_OK:
+        raise ThyError(code, what)
+
+
+def _p(a, t):
+    return ctypes.cast(None, t) if a is None else a.ctypes.data_as(t)
+
+
+def device_count() -> int:
+    return int(_ffi.lib().thy_device_count())
+
+
+class Prepared:
+    """A dimensionless problem (thy_problem) owned by the library."""
+
+    def __init__(self, problem: "synth.Problem"):
+        L = _ffi.lib()
+        self.problem = problem
+        self._keep = []
+        raw = _ffi.Raw()
+        raw.nx, raw.ny = problem.nx, problem.ny
+        lon = np.ascontiguousarray(problem.lon, np.float64)
+        lat = np.ascontiguousarray(problem.lat, np.float64)
+        z = np.ascontiguousarray(problem.z, np.float32)
+        self._keep += [lon, lat, z]
+        raw.lon, raw.lat, raw.z = _p(lon, _ffi.f64p), _p(lat, _ffi.f64p), _p(z, _ffi.f32p)
+        if problem.faults:
+            f = np.ascontiguousarray(problem.fault_array(), np.float64)
+            self._keep.append(f)
+            raw.nfaults, raw.faults = len(problem.faults), _p(f, _ffi.f64p)
+            raw.eta_file = _p(None, _ffi.f32p)
+        else:
+            e = np.ascontiguousarray(np.zeros_like(z) if problem.eta_init is None else problem.eta_init, np.float32)
+            self._keep.append(e)
+            raw.eta_file = _p(e, _ffi.f32p)
+            raw.nfaults, raw.faults = 0, _p(None, _ffi.f64p)
+        raw.crop_flag, raw.crop_value = int(problem.crop_flag), float(problem.crop_value)
+        for i in range(4):
+            raw.borders[i] = float(problem.borders[i])
+        raw.sim_time, raw.save_time = float(problem.sim_time), float(problem.save_time)
+        if problem.points is not None and len(problem.points) > 0:
+            pts = np.ascontiguousarray(problem.points, np.float64)
+            self._keep.append(pts)
+            raw.npoints, raw.points, raw.series_time = len(pts), _p(pts, _ffi.f64p), float(problem.series_time)
+        else:
+            raw.npoints, raw.points, raw.series_time = 0, _p(None, _ffi.f64p), -1.0
+        raw.cfl, raw.eps_h, raw.hpos, raw.stability = problem.cfl, problem.eps_h, problem.hpos, problem.stability
+        raw.manning, raw.vmax, raw.L, raw.H, raw.dif_at = (problem.manning, problem.vmax, problem.L, problem.H,
+                                                           problem.dif_at)
+        self._raw = raw
+        h = ctypes.c_void_p()
+        _check(L.thy_prepare(ctypes.byref(raw), ctypes.byref(h)), "thy_prepare")
+        self._h = h
+        self.view = L.thy_problem_view(h)
+
+    @property
+    def c(self) -> "_ffi.ProblemC":
+        return self.view.contents
+
+    @property
+    def npoints(self) -> int:
+        return int(self.c.npoints)
+
+    def __del__(self):
+        try:
+            if getattr(self, "_h", None):
+                _ffi.lib().thy_problem_free(self._h)
+        except Exception:
+            pass
+
+
+def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = True) -> Dict:
+    """Runs one scenario end to end on the GPU through thy_run()."""
+    L = _ffi.lib()
+    prep = problem if isinstance(problem, Prepared) else Prepared(problem)
+    pc = prep.c
+    pc.max_steps = max_steps
+    ny, nx = pc.ny, pc.nx
+    fields = {k: np.empty((ny, nx), np.float32) for k in ("max_height", "arrival", "deformed_bathy", "eta", "ux", "uy")}
+    npts = max(pc.npoints, 1)
+    pts = {k: np.empty(npts, np.float32) for k in ("series_min", "series_max", "series_bathy")}
+    snaps = {"time": [], "eta": [], "ux": [], "uy": []}
+    ser = {"time": [], "eta": [], "ux": [], "uy": []}
+
+    def on_snap(user, idx, t, e, u, v):
+        n = nx * ny
+        snaps["time"].append(t)
+        snaps["eta"].append(np.ctypeslib.as_array(e, (n,)).reshape(ny, nx).copy())
+        snaps["ux"].append(np.ctypeslib.as_array(u, (n,)).reshape(ny, nx).copy())
+        snaps["uy"].append(np.ctypeslib.as_array(v, (n,)).reshape(ny, nx).copy())
+
+    def on_ser(user, idx, t, e, u, v):
+        n = pc.npoints
+        ser["time"].append(t)
+        ser["eta"].append(np.ctypeslib.as_array(e, (n,)).copy())
+        ser["ux"].append(np.ctypeslib.as_array(u, (n,)).copy())
+        ser["uy"].append(np.ctypeslib.as_array(v, (n,)).copy())
+
+    o = _ffi.Outputs()
+    for k, v in fields.items():
+        setattr(o, k, _p(v, _ffi.f32p))
+    for k, v in pts.items():
+        setattr(o, k, _p(v, _ffi.f32p))
+    cb_snap = _ffi.FieldFn(on_snap) if snapshots else _ffi.FieldFn()
+    cb_ser = _ffi.FieldFn(on_ser) if series else _ffi.FieldFn()
+    o.on_snapshot, o.on_series, o.user = cb_snap, cb_ser, None
+    st = _ffi.Stats()
+    _check(L.thy_run(prep.view, ctypes.byref(o), ctypes.byref(st)), "thy_run")
+    res: Dict = dict(fields)
+    res["snapshots"] = {k: (np.asarray(v) if v else np.empty((0,))) for k, v in snaps.items()}
+    res["series"] = {k: (np.asarray(v) if v else np.empty((0,))) for k, v in ser.items()}
+    res["series"].update(min=pts["series_min"][:pc.npoints], max=pts["series_max"][:pc.npoints],
+                         bathy=pts["series_bathy"][:pc.npoints])
+    res.update(iterations=st.steps, final_time=st.final_time_s, first_dt=st.first_dt_s,
+               loop_seconds=st.loop_seconds, device_ms=st.device_loop_ms, kernel_launches=st.kernel_launches,
+               nsnaps=st.snapshots, nseries=st.series_samples)
+    return res
+
+
+class Session:
+    """Step-level access (thy_session_*): the problem is set up on the device
+    (faults at t=0 applied), then any number of time steps can be timed."""
+
+    def __init__(self, problem):
+        L = _ffi.lib()
+        self.prep = problem if isinstance(problem, Prepared) else Prepared(problem)
+        h = ctypes.c_void_p()
+        _check(L.thy_session_open(self.prep.view, ctypes.byref(h)), "thy_session_open")
+        self._h = h
+        self.cells = self.prep.c.nx * self.prep.c.ny
+
+    def steps(self, k: int):
+        """Runs k steps; returns (device milliseconds, steps done)."""
+        ms = ctypes.c_double()
+        done = ctypes.c_longlong()
+        _check(_ffi.lib().thy_session_steps(self._h, k, ctypes.byref(ms), ctypes.byref(done)), "thy_session_steps")
+        return ms.value, done.value
+
+    def time(self) -> float:
+        return float(_ffi.lib().thy_session_time(self._h))
+
+    def fetch(self):
+        c = self.prep.c
+        out = {k: np.empty((c.ny, c.nx), np.float32) for k in ("max_height", "eta", "ux", "uy")}
+        _check(_ffi.lib().thy_session_fetch(self._h, *(_p(out[k], _ffi.f32p) for k in ("max_height", "eta", "ux", "uy"))),
+               "thy_session_fetch")
+        return out
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _ffi.lib().thy_session_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
