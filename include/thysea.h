@@ -159,6 +159,10 @@ typedef struct thy_session thy_session;
 int thy_session_open(const thy_problem *p, thy_session **out);
 int thy_session_steps(thy_session *s, long long steps, double *device_ms, long long *steps_done);
 int thy_session_fetch(thy_session *s, float *max_height, float *eta, float *ux, float *uy);
+/* average device time (ms) of the phase-1 (mass + diagnostics) and phase-2
+ * (momentum + dt) launches over `steps` individually launched steps */
+int thy_session_profile(thy_session *s, long long steps, double *phase1_ms, double *phase2_ms);
+long long thy_session_launches(const thy_session *s);   /* stepping kernels launched so far */
 double thy_session_time(const thy_session *s);    /* simulated time (s) */
 void thy_session_close(thy_session *s);
 

@@ -84,7 +84,42 @@ def refemu_lib():
         _ref.refemu_run.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_int, _f64p]
         _ref.refemu_run.restype = ctypes.c_int
         _ref.refemu_okada_points.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p, _f64p]
+        _ref.refemu_open.argtypes = [ctypes.c_char_p, ctypes.c_int]
+        _ref.refemu_open.restype = ctypes.c_void_p
+        _ref.refemu_steps.argtypes = [ctypes.c_void_p, ctypes.c_longlong]
+        _ref.refemu_steps.restype = ctypes.c_double
+        _ref.refemu_cells.argtypes = [ctypes.c_void_p]
+        _ref.refemu_cells.restype = ctypes.c_longlong
+        _ref.refemu_close.argtypes = [ctypes.c_void_p]
     return _ref
+
+
+class RefemuSession:
+    """The reference's own loop body on the host, step by step (for timing)."""
+
+    def __init__(self, txt_path: str, threads: int = 0):
+        self.lib = refemu_lib()
+        self.h = self.lib.refemu_open(txt_path.encode(), threads)
+        if not self.h:
+            raise RuntimeError(f"refemu_open failed for {txt_path}")
+        self.cells = int(self.lib.refemu_cells(self.h))
+
+    def steps(self, k: int) -> float:
+        s = float(self.lib.refemu_steps(self.h, k))
+        if s < 0:
+            raise RuntimeError("refemu_steps failed")
+        return s
+
+    def close(self):
+        if self.h:
+            self.lib.refemu_close(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def _ptr(a: Optional[np.ndarray], ctype):

@@ -467,6 +467,122 @@ extern "C" int refemu_run(const char *txt, long long max_iterations, int threads
     return err;
 }
 
+// ---- step-level session (bench.py's reference arm / CPU baseline) -----
+// Loads a problem file with the reference's loader, allocates the state,
+// computes the initial dt and applies the faults due at t = 0 (the first
+// actions of the reference's loop); refemu_steps then times whole loop
+// iterations (metrics update + siguientePasoNivel0 + dt truncation), without
+// NetCDF output.
+struct RefemuSession {
+    int nx = 0, ny = 0, nF = 0, crop = 0, fault = 0;
+    bool per = false, saltar = false;
+    double bs, bi, bl, br, Hmin, eps, difat, mf0, vmax, CFL, hpos, cvis, L, H, Q, T, crop_v, tt, t = 0, dt = 0;
+    int sS, sI, sL, sR;
+    double LON_C[MAX_FAULTS], LAT_C[MAX_FAULTS], DEPTH_C[MAX_FAULTS], FL[MAX_FAULTS], FW[MAX_FAULTS];
+    double STR[MAX_FAULTS], DIPA[MAX_FAULTS], RAKE[MAX_FAULTS], SLIP[MAX_FAULTS], defT[MAX_FAULTS];
+    double2 *h1 = nullptr, *h2 = nullptr, *a1 = nullptr, *a2 = nullptr;
+    double *etaMax = nullptr, *tLleg = nullptr, *etaIni = nullptr, *dT = nullptr;
+    float *vec = nullptr;
+    tipoDatosSubmalla dn;
+    dim3 gV1, gV2, gH1, gH2, gE, tA, tE;
+    long long steps = 0;
+};
+
+extern "C" void *refemu_open(const char *txt, int threads)
+{
+    if (threads > 0) omp_set_num_threads(threads);
+    auto *S = new RefemuSession();
+    std::memset(&S->dn, 0, sizeof(S->dn));
+    int *pos = nullptr, leer, nP, nNiv, okada;
+    double *lonP = nullptr, *latP = nullptr, tnc, tts;
+    int64_t N;
+    std::string nombre, prefijo;
+    int err = cargarDatosProblema(txt, nombre, prefijo, &nNiv, &okada, &S->nF, &S->crop, &S->crop_v, S->LON_C, S->LAT_C,
+                                  S->DEPTH_C, S->FL, S->FW, S->STR, S->DIPA, S->RAKE, S->SLIP, S->defT, &S->h1, &S->h2,
+                                  &S->dn, &S->nx, &S->ny, &N, &leer, &nP, &pos, &lonP, &latP, &S->Hmin, &S->bs, &S->bi,
+                                  &S->bl, &S->br, &S->sS, &S->sI, &S->sL, &S->sR, &S->tt, &tnc, &tts, &S->CFL, &S->mf0,
+                                  &S->vmax, &S->eps, &S->hpos, &S->cvis, &S->difat, &S->L, &S->H, &S->Q, &S->T);
+    if (err > 0) {
+        delete S;
+        return nullptr;
+    }
+    free(pos); free(lonP); free(latP);
+    const long long n = (long long)S->nx * S->ny;
+    S->per = (fabs(S->bl - 2.0) < EPSILON) && (fabs(S->br - 2.0) < EPSILON);
+    emuTamBloques(S->nx, S->ny, &S->gV1, &S->gV2, &S->gH1, &S->gH2, &S->gE);
+    S->tA = dim3(NUM_HEBRASX_ARI, NUM_HEBRASY_ARI);
+    S->tE = dim3(NUM_HEBRASX_EST, NUM_HEBRASY_EST);
+    S->a1 = (double2 *)calloc(n, sizeof(double2));
+    S->a2 = (double2 *)calloc(n, sizeof(double2));
+    S->etaMax = (double *)malloc(n * sizeof(double));
+    S->tLleg = (double *)malloc(n * sizeof(double));
+    S->etaIni = (double *)malloc(n * sizeof(double));
+    S->dT = (double *)malloc(n * sizeof(double));
+    S->vec = (float *)malloc(n * sizeof(float));
+    int nx = S->nx, ny = S->ny;
+    emu_launch(S->gE, S->tE, [&] { inicializarEta1MaximaNivel0GPU(S->h1, S->etaMax, nx, ny, S->eps); });
+    emu_launch(S->gE, S->tE, [&] { inicializarEta1MaximaNivel0GPU(S->h1, S->etaIni, nx, ny, S->eps); });
+    emu_launch(S->gE, S->tE, [&] { inicializarTiemposLlegadaNivel0GPU(S->tLleg, nx, ny); });
+    S->dt = emuDeltaTInicial(S->h1, S->h2, &S->dn, S->dT, S->a1, nx, ny, S->bl, S->br, S->bs, S->bi, S->per, S->CFL,
+                             S->eps, S->gV1, S->gV2, S->gH1, S->gH2, S->tA, S->gE, S->tE);
+    if (S->nF > 0) {
+        if (S->defT[0] < EPSILON) emuTruncarSaltando(S->nF, S->fault, S->t, S->defT, S->T, &S->dt, &S->saltar);
+        else emuTruncar(S->nF, S->fault, S->t, S->defT, S->T, &S->dt, &S->saltar);
+    }
+    memset(S->a1, 0, n * sizeof(double2));
+    double lon_ini = S->dn.longitud[0], lat_ini = S->dn.latitud[0];
+    double incx = (S->dn.longitud[nx - 1] - lon_ini) / (nx - 1), incy = (S->dn.latitud[ny - 1] - lat_ini) / (ny - 1);
+    while (S->fault < S->nF && S->t * S->T >= S->defT[S->fault]) {
+        int f = S->fault;
+        emuAplicarOkada(S->h1, S->etaIni, S->crop, S->crop_v, S->dT, S->vec, nx, ny, lon_ini, incx, lat_ini, incy,
+                        S->LON_C[f], S->LAT_C[f], S->DEPTH_C[f], S->FL[f], S->FW[f], S->STR[f], S->DIPA[f], S->RAKE[f],
+                        S->SLIP[f], S->gE, S->tE, S->H);
+        S->fault++;
+    }
+    return S;
+}
+
+// Runs k loop iterations; returns their wall seconds (negative on error).
+extern "C" double refemu_steps(void *handle, long long k)
+{
+    auto *S = (RefemuSession *)handle;
+    if (!S) return -1.0;
+    const int nx = S->nx, ny = S->ny;
+    const long long nb2 = (long long)nx * ny * (long long)sizeof(double2);
+    auto t0 = std::chrono::high_resolution_clock::now();
+    for (long long i = 0; i < k; i++) {
+        double t = S->t;
+        emu_launch(S->gE, S->tE, [&] { actualizarEta1MaximaNivel0GPU(S->h1, S->etaMax, nx, ny, t, S->eps); });
+        emu_launch(S->gE, S->tE, [&] { actualizarTiemposLlegadaNivel0GPU(S->h1, S->tLleg, S->etaIni, nx, ny, t, S->difat); });
+        S->dt = emuSiguientePaso(S->h1, S->h2, &S->dn, S->a1, S->a2, nx, ny, S->dT, S->bs, S->bi, S->bl, S->br, S->per,
+                                 S->Hmin, S->sS, S->sI, S->sL, S->sR, SEA_LEVEL / S->H, &S->t, S->CFL, S->dt, S->mf0,
+                                 S->vmax, S->eps, S->hpos, S->cvis, nb2, S->gV1, S->gV2, S->gH1, S->gH2, S->tA, S->gE,
+                                 S->tE);
+        if (!S->saltar) emuTruncar(S->nF, S->fault, S->t, S->defT, S->T, &S->dt, &S->saltar);
+        else emuTruncarSaltando(S->nF, S->fault, S->t, S->defT, S->T, &S->dt, &S->saltar);
+        memset(S->a1, 0, nb2);
+        memset(S->a2, 0, nb2);
+        S->steps++;
+    }
+    auto t1 = std::chrono::high_resolution_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+extern "C" long long refemu_cells(void *handle)
+{
+    auto *S = (RefemuSession *)handle;
+    return S ? (long long)S->nx * S->ny : 0;
+}
+
+extern "C" void refemu_close(void *handle)
+{
+    auto *S = (RefemuSession *)handle;
+    if (!S) return;
+    liberarMemoria(S->h1, S->h2, S->dn, nullptr, nullptr, nullptr);
+    free(S->a1); free(S->a2); free(S->etaMax); free(S->tLleg); free(S->etaIni); free(S->dT); free(S->vec);
+    delete S;
+}
+
 // Okada vertical displacement (meters) at arbitrary points, via the
 // reference's prtoxy_ + dc3d_ exactly as aplicarOkadaStandardGPU calls them.
 extern "C" void refemu_okada_points(int n, const double *lon, const double *lat, const double *fault, double *uz)

@@ -37,6 +37,9 @@ CUDA_SOURCES = [
     "host/problem.cpp",
 ]
 C_SOURCES = ["nclite/nclite.c"]
+# FP32 stepping kernels: approximate division / sqrt / exp (<= 2 ulp); the FP64
+# Okada and set-up kernels keep IEEE arithmetic
+FAST_MATH = {"kernels/step.cu"}
 
 
 def _obj(src: str) -> str:
@@ -73,6 +76,8 @@ def _compile(src: str, verbose: bool) -> str:
         if src.endswith(".cpp"):
             cmd.insert(1, "-x")
             cmd.insert(2, "cu")
+        if src in FAST_MATH:
+            cmd.insert(1, "-use_fast_math")
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
     r = subprocess.run(cmd, capture_output=True, text=True)

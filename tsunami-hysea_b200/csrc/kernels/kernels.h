@@ -8,9 +8,9 @@ namespace thy {
 
 struct ScenarioDev;
 
-constexpr int kTileX = 32;        // tile width (cells)
-constexpr int kTileY = 16;        // tile height (cells)
-constexpr int kStepThreads = 256;
+constexpr int kStepThreads = 128;           // 4 warps = 4 column strips per tile
+constexpr int kTileX = 28 * (kStepThreads / 32);   // tile width: 28 output columns per warp
+constexpr int kTileY = 32;                  // tile height: rows one warp marches through
 
 // step.cu
 size_t step_smem_bytes();

@@ -656,6 +656,49 @@ extern "C" int thy_session_steps(thy_session *S, long long steps, double *device
     return s.hctl.status == kFailed ? THY_ERR_NONFINITE : THY_OK;
 }
 
+// Per-kernel device time: `steps` steps launched one kernel at a time with
+// CUDA events around each launch on the session's stream.  Returns the
+// average duration (ms) of the phase-1 and phase-2 launches.
+extern "C" int thy_session_profile(thy_session *S, long long steps, double *phase1_ms, double *phase2_ms)
+{
+    if (!S || steps <= 0) return THY_ERR_INVALID;
+    DevScenario &s = S->s;
+    Batch &b = S->b;
+    int rc;
+    s.hctl.max_steps = s.hctl.step + steps;
+    s.hctl.status = kRunning;
+    s.hctl.events = 0;
+    if ((rc = s.upload_ctl(S->st))) return rc;
+    std::vector<cudaEvent_t> ev(3 * steps);
+    for (auto &e : ev) THY_CK(cudaEventCreate(&e));
+    for (long long k = 0; k < steps; k++) {
+        THY_CK(cudaEventRecord(ev[3 * k], S->st));
+        launch_step_phase(1, b.d_table, b.d_work, b.d_nwork, b.grid, S->st);
+        THY_CK(cudaEventRecord(ev[3 * k + 1], S->st));
+        launch_step_phase(2, b.d_table, b.d_work, b.d_nwork, b.grid, S->st);
+        THY_CK(cudaEventRecord(ev[3 * k + 2], S->st));
+    }
+    THY_CK(cudaGetLastError());
+    THY_CK(cudaStreamSynchronize(S->st));
+    double t1 = 0, t2 = 0;
+    for (long long k = 0; k < steps; k++) {
+        float a = 0, c = 0;
+        THY_CK(cudaEventElapsedTime(&a, ev[3 * k], ev[3 * k + 1]));
+        THY_CK(cudaEventElapsedTime(&c, ev[3 * k + 1], ev[3 * k + 2]));
+        t1 += a;
+        t2 += c;
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    b.launches += 2 * steps;
+    if ((rc = s.download_ctl(S->st))) return rc;
+    THY_CK(cudaStreamSynchronize(S->st));
+    if (phase1_ms) *phase1_ms = t1 / steps;
+    if (phase2_ms) *phase2_ms = t2 / steps;
+    return s.hctl.status == kFailed ? THY_ERR_NONFINITE : THY_OK;
+}
+
+extern "C" long long thy_session_launches(const thy_session *S) { return S ? S->b.launches : 0; }
+
 extern "C" int thy_session_fetch(thy_session *S, float *max_height, float *eta, float *ux, float *uy)
 {
     if (!S) return THY_ERR_INVALID;

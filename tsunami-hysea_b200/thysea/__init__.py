@@ -170,6 +170,15 @@ class Session:
     def time(self) -> float:
         return float(_ffi.lib().thy_session_time(self._h))
 
+    def profile(self, k: int):
+        """k individually launched steps; returns the average (phase-1 ms, phase-2 ms)."""
+        a, b = ctypes.c_double(), ctypes.c_double()
+        _check(_ffi.lib().thy_session_profile(self._h, k, ctypes.byref(a), ctypes.byref(b)), "thy_session_profile")
+        return a.value, b.value
+
+    def launches(self) -> int:
+        return int(_ffi.lib().thy_session_launches(self._h))
+
     def fetch(self):
         c = self.prep.c
         out = {k: np.empty((c.ny, c.nx), np.float32) for k in ("max_height", "eta", "ux", "uy")}

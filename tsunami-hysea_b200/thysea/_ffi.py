@@ -93,6 +93,8 @@ SIGNATURES = {
                           ctypes.c_int),
     "thy_session_fetch": ([ctypes.c_void_p, f32p, f32p, f32p, f32p], ctypes.c_int),
     "thy_session_time": ([ctypes.c_void_p], ctypes.c_double),
+    "thy_session_profile": ([ctypes.c_void_p, ctypes.c_longlong, f64p, f64p], ctypes.c_int),
+    "thy_session_launches": ([ctypes.c_void_p], ctypes.c_longlong),
     "thy_session_close": ([ctypes.c_void_p], None),
 }
 
