@@ -152,6 +152,20 @@ int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *stats);
  * with gauges, <prefix>_ts.nc (src/GPU/netcdfTH.cu, src/GPU/netcdfSeries.cu). */
 int thy_run_netcdf(const thy_problem *p, const char *problem_name, const char *prefix, thy_stats *stats);
 
+/* The Okada stage alone on device memory, replacing
+ *   void aplicarOkada(...)                       src/GPU/Deformacion.cu:118-143
+ * d_state1 is the reference's device state (double2 (h, H) per cell,
+ * dimensionless, nx*ny), d_eta_initial its eta_initial field (may be NULL);
+ * fault holds the 10 problem-file values (time lon lat depth_km length_km
+ * width_km strike dip rake slip_m); the stations are lon0 + i*dlon,
+ * lat0 + j*dlat; H is the depth scale; crop_flag / crop_value as in
+ * thy_problem.  Computes U_Z in FP64, crops, then H -= U_Z/H_scale and
+ * eta_initial += U_Z/H_scale.  Runs on the caller's current device and
+ * `stream` (a cudaStream_t, NULL = default stream); allocates its nx*ny
+ * doubles of scratch with cudaMalloc and returns after the stream is idle. */
+int thy_apply_okada(int nx, int ny, double lon0, double dlon, double lat0, double dlat, const double *fault,
+                    double H, int crop_flag, double crop_value, void *d_state1, double *d_eta_initial, void *stream);
+
 /* Step-level access for benchmarking: set up a problem on the device, run
  * `steps` time steps (Okada applied first), report the device time of the
  * stepping kernels.  No outputs are produced. */

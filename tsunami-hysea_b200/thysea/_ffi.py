@@ -88,6 +88,9 @@ SIGNATURES = {
     "thy_run": ([ctypes.POINTER(ProblemC), ctypes.POINTER(Outputs), ctypes.POINTER(Stats)], ctypes.c_int),
     "thy_run_netcdf": ([ctypes.POINTER(ProblemC), ctypes.c_char_p, ctypes.c_char_p, ctypes.POINTER(Stats)],
                        ctypes.c_int),
+    "thy_apply_okada": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                         ctypes.c_double, f64p, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
+                         ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "thy_session_open": ([ctypes.POINTER(ProblemC), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "thy_session_steps": ([ctypes.c_void_p, ctypes.c_longlong, f64p, ctypes.POINTER(ctypes.c_longlong)],
                           ctypes.c_int),
