@@ -42,6 +42,7 @@ extern "C" {
 #define THY_ERR_NONFINITE 6    /* the state or the time step became non-finite */
 #define THY_ERR_BUDGET 7       /* a scenario does not fit the server's HBM budget */
 #define THY_ERR_CANCELLED 8    /* a served request was cancelled */
+#define THY_ERR_TOO_LARGE 9    /* grid larger than an allocation-free entry point's fixed scratch */
 
 /* ------------------------------------------------------------------------
  * Raw problem: the contents of the problem .txt file and of its GRD and
@@ -165,6 +166,21 @@ int thy_run_netcdf(const thy_problem *p, const char *problem_name, const char *p
  * doubles of scratch with cudaMalloc and returns after the stream is idle. */
 int thy_apply_okada(int nx, int ny, double lon0, double dlon, double lat0, double dlat, const double *fault,
                     double H, int crop_flag, double crop_value, void *d_state1, double *d_eta_initial, void *stream);
+
+/* thy_apply_okada without any device allocation.  No counterpart in the
+ * reference: it serves callers that cannot call cudaMalloc (the GPU's memory
+ * is owned by a caching or budgeted allocator, or an allocation's implicit
+ * device-wide synchronisation is not allowed where they run).  Its scratch
+ * is a fixed array inside the library, THY_OKADA_NOALLOC_MAX_CELLS doubles
+ * (8 MiB) held by every GPU that loads the library until the process exits;
+ * larger grids return THY_ERR_TOO_LARGE.  The first call on a device looks
+ * up that array's device address, so it should come before any stream
+ * capture.  The call only enqueues the work on `stream`.  All calls share
+ * the scratch: calls whose work overlaps on the GPU race. */
+#define THY_OKADA_NOALLOC_MAX_CELLS (1 << 20)
+int thy_apply_okada_noalloc(int nx, int ny, double lon0, double dlon, double lat0, double dlat, const double *fault,
+                            double H, int crop_flag, double crop_value, void *d_state1, double *d_eta_initial,
+                            void *stream);
 
 /* Step-level access for benchmarking: set up a problem on the device, run
  * `steps` time steps (Okada applied first), report the device time of the

@@ -530,6 +530,7 @@ extern "C" const char *thy_strerror(int code)
     case THY_ERR_NONFINITE: return "the state or the time step became non-finite";
     case THY_ERR_BUDGET: return "scenario does not fit the HBM budget";
     case THY_ERR_CANCELLED: return "request cancelled";
+    case THY_ERR_TOO_LARGE: return "grid exceeds the allocation-free entry point's maximum of 1048576 cells";
     default: return "unknown error";
     }
 }

@@ -3,9 +3,29 @@
 // layout (double2 (h, H) per cell, dimensionless): the FP64 vertical
 // deformation of one fault, optional relative / absolute cropping, then
 // H -= U_Z and eta_initial += U_Z (src/GPU/Deformacion.cu:38-53).
+//
+// Two entry points run the same kernels and differ only in where the
+// scratch (the nx*ny deformation field and one word for the cropping
+// maximum) lives: thy_apply_okada takes it from cudaMalloc for the call;
+// thy_apply_okada_noalloc uses the fixed-size device arrays below, for
+// callers that must not allocate device memory at all.
+#include <mutex>
+
 #include "engine.h"
 
 namespace thy {
+
+// Scratch of thy_apply_okada_noalloc.  File-scope device arrays: every GPU
+// that loads the library holds them (8 MiB + 4 bytes) until the process
+// exits, and every call shares them.
+static __device__ __align__(256) double g_okada_scratch[THY_OKADA_NOALLOC_MAX_CELLS];
+static __device__ __align__(256) unsigned int g_okada_scratch_max;
+
+namespace {
+std::mutex g_scratch_mu;
+double *g_scratch_dev[64] = {};        // device address of g_okada_scratch, per device
+unsigned int *g_max_dev[64] = {};      // device address of g_okada_scratch_max, per device
+}  // namespace
 
 __global__ void okada_kernel(int nx, int ny, double *__restrict__ def, double lon0, double dlon, double lat0,
                              double dlat, OkadaFault f, double Hs);
@@ -84,4 +104,43 @@ extern "C" int thy_apply_okada(int nx, int ny, double lon0, double dlon, double 
     if (rc) return rc;
     THY_CK(e);
     return THY_OK;
+}
+
+// Same computation with the library's fixed device scratch instead of a
+// cudaMalloc: for callers that cannot allocate device memory (a caching or
+// budgeted allocator owns the GPU, or an allocation's implicit device-wide
+// synchronisation is not acceptable).  Up to THY_OKADA_NOALLOC_MAX_CELLS
+// cells; larger grids return THY_ERR_TOO_LARGE before any work.  The first
+// call on a device looks up the scratch's device address there
+// (cudaGetSymbolAddress), so make that first call before any stream capture.
+// The work is only enqueued on `stream`.  The scratch is shared by every
+// call and keeps the last call's contents (the cropping maximum is cleared
+// at the start of each call); calls whose work overlaps on the GPU (other
+// streams, other host threads) race on it.
+extern "C" int thy_apply_okada_noalloc(int nx, int ny, double lon0, double dlon, double lat0, double dlat,
+                                       const double *fault, double H, int crop_flag, double crop_value,
+                                       void *d_state1, double *d_eta_initial, void *stream)
+{
+    int rc = check_okada_args(nx, ny, fault, crop_flag, d_state1);
+    if (rc) return rc;
+    if ((long long)nx * ny > (long long)THY_OKADA_NOALLOC_MAX_CELLS) return THY_ERR_TOO_LARGE;
+    int dev = 0;
+    THY_CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 64) return THY_ERR_INVALID;
+    double *def;
+    unsigned int *mx;
+    {
+        std::lock_guard<std::mutex> lock(g_scratch_mu);
+        if (!g_scratch_dev[dev]) {
+            void *a = nullptr, *b = nullptr;
+            THY_CK(cudaGetSymbolAddress(&a, g_okada_scratch));
+            THY_CK(cudaGetSymbolAddress(&b, g_okada_scratch_max));
+            g_scratch_dev[dev] = (double *)a;
+            g_max_dev[dev] = (unsigned int *)b;
+        }
+        def = g_scratch_dev[dev];
+        mx = g_max_dev[dev];
+    }
+    return enqueue_okada_reference_layout(nx, ny, lon0, dlon, lat0, dlat, fault, H, crop_flag, crop_value,
+                                          (double2 *)d_state1, d_eta_initial, def, mx, (cudaStream_t)stream);
 }

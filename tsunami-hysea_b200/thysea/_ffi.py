@@ -91,6 +91,9 @@ SIGNATURES = {
     "thy_apply_okada": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
                          ctypes.c_double, f64p, ctypes.c_double, ctypes.c_int, ctypes.c_double, ctypes.c_void_p,
                          ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
+    "thy_apply_okada_noalloc": ([ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                                 ctypes.c_double, f64p, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p], ctypes.c_int),
     "thy_session_open": ([ctypes.POINTER(ProblemC), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "thy_session_steps": ([ctypes.c_void_p, ctypes.c_longlong, f64p, ctypes.POINTER(ctypes.c_longlong)],
                           ctypes.c_int),
