@@ -49,19 +49,24 @@ def env_int(k, d):
 
 
 class Dist:
-    def __init__(self):
+    """torch.distributed plumbing of the replicas: barrier, max and sum over
+    ranks (NCCL on GPUs, gloo for CPU tests)."""
+
+    def __init__(self, backend: str = "nccl"):
         self.world = env_int("WORLD_SIZE", 1)
         self.rank = env_int("RANK", 0)
         self.local = env_int("LOCAL_RANK", 0)
         self.pg = None
+        self.device = "cuda" if backend == "nccl" else "cpu"
         if self.world > 1:
             import datetime
 
             import torch
             import torch.distributed as dist
 
-            torch.cuda.set_device(self.local)
-            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+            if backend == "nccl":
+                torch.cuda.set_device(self.local)
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
             self.pg = dist
 
     def barrier(self):
@@ -73,7 +78,7 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX)
         return float(t.item())
 
@@ -82,7 +87,7 @@ class Dist:
             return v
         import torch
 
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        t = torch.tensor([v], dtype=torch.float64, device=self.device)
         self.pg.all_reduce(t, op=self.pg.ReduceOp.SUM)
         return float(t.item())
 
