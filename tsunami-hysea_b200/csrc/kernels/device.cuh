@@ -118,10 +118,13 @@ __device__ __forceinline__ float monotone_limiter(float pm, float p0, float p1, 
 
 // Limits a mass flux so that neither side loses more than 1/4 of its water in
 // one step (src/GPU/Arista_kernel.cu:79-114; c0/c1 = cos(lat) for y edges).
+// dt > dt0 = cap / (|F| + eps) is tested as dt (|F| + eps) > cap, so the
+// divisions only run when the limit applies.
 __device__ __forceinline__ float limit_outflow(float F, float h0, float h1, float c0, float c1, float dt, float a0, float a1)
 {
-    float dt0 = (F > 0.f) ? 0.25f * h0 * c0 * a0 / (F + kEps) : 0.25f * h1 * c1 * a1 / (-F + kEps);
-    if (dt > dt0) F *= dt0 / (dt + kEps);
+    const float cap = (F > 0.f) ? 0.25f * h0 * c0 * a0 : 0.25f * h1 * c1 * a1;
+    const float aF = fabsf(F) + kEps;
+    if (dt * aF > cap) F *= (cap / aF) / (dt + kEps);
     return F;
 }
 

@@ -16,8 +16,8 @@
 // row needs nothing but that window; x edges take their left/right
 // neighbours from warp shuffles.  The 32 lanes cover 28 output columns plus
 // a two-column halo on each side (the x stencil reaches two cells), so the
-// loads of a strip are whole rows and need no shared memory.  The next row is
-// loaded while the current one is computed.  Each edge flux is evaluated once
+// loads of a strip are whole rows and need no shared memory.  Rows are
+// loaded two ahead of the one being computed.  Each edge flux is evaluated once
 // per strip: the lane right of an x edge computes it and hands the left
 // cell's share to its neighbour with one shuffle; the y edge below row y is
 // carried to row y+1 in registers.  No accumulator arrays, no edge
@@ -68,6 +68,33 @@ __device__ __forceinline__ Cell load_cell(const float *__restrict__ eta, const f
     c.qx = __ldg(qx + idx);
     c.qy = __ldg(qy + idx);
     c.h = c.e + c.D;
+    return c;
+}
+
+// raw loads of a row that is still in flight (prefetch two rows ahead)
+struct RawCell {
+    float e, D, qx, qy;
+};
+
+__device__ __forceinline__ RawCell load_raw(const float *__restrict__ eta, const float *__restrict__ dep,
+                                            const float *__restrict__ qx, const float *__restrict__ qy, size_t idx)
+{
+    RawCell r;
+    r.e = __ldg(eta + idx);
+    r.D = __ldg(dep + idx);
+    r.qx = __ldg(qx + idx);
+    r.qy = __ldg(qy + idx);
+    return r;
+}
+
+__device__ __forceinline__ Cell finish(const RawCell &r)
+{
+    Cell c;
+    c.e = r.e;
+    c.D = r.D;
+    c.qx = r.qx;
+    c.qy = r.qy;
+    c.h = r.e + r.D;
     return c;
 }
 
@@ -245,13 +272,14 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
             Cell c2 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0, ny) * pitch + col);
             Cell c3 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 + 1, ny) * pitch + col);
             Cell c4 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 + 2, ny) * pitch + col);
+            RawCell n1 = load_raw(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 + 3, ny) * pitch + col);
             // y edge at the top of the first row (stencil rows y0-2 .. y0+1)
             Contrib top, dummy;
             y_edge<PHASE>(s, c0, c1, c2, c3, y0, dt, dummy, top);
 
             for (int yo = y0; yo < y_end; yo++) {
-                // next row of the window, in flight while this row is computed
-                const Cell nxt = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(yo + 3, ny) * pitch + col);
+                // rows yo+3 (loaded an iteration ago) and yo+4 (now) are in flight
+                const RawCell n2 = load_raw(eta_in, s.dep, qx_in, qy_in, clamp_row(yo + 4, ny) * pitch + col);
                 const size_t idx = (size_t)yo * pitch + col;
                 float em = 0.f, ar = 0.f, ei = 0.f;
                 if (PHASE == 1 && has_cell) {
@@ -272,16 +300,21 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                 e.h1 = c2.h;
                 e.u1 = c2.qx;
                 if (PHASE != 0) {
-                    e.v0m = shup(c2.qy, 2);
                     e.e0 = shup(c2.e, 1);
                     e.D0 = shup(c2.D, 1);
-                    e.v0 = shup(c2.qy, 1);
                     e.h1p = shdn(c2.h, 1);
                     e.e1p = shdn(c2.e, 1);
-                    e.v1p = shdn(c2.qy, 1);
                     e.e1 = c2.e;
                     e.D1 = c2.D;
+                }
+                if (PHASE == 2) {
+                    // the tangential discharge only enters the momentum flux
+                    e.v0m = shup(c2.qy, 2);
+                    e.v0 = shup(c2.qy, 1);
+                    e.v1p = shdn(c2.qy, 1);
                     e.v1 = c2.qy;
+                } else {
+                    e.v0m = e.v0 = e.v1p = e.v1 = 0.f;
                 }
                 e.u0m = e.u1p = 0.f;
                 const float area = __ldg(s.row.area + yo);
@@ -421,7 +454,8 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                 c1 = c2;
                 c2 = c3;
                 c3 = c4;
-                c4 = nxt;
+                c4 = finish(n1);
+                n1 = n2;
             }
         }
         if (bad) atomicOr(&ctl->errors, 1u);
