@@ -7,8 +7,9 @@ Workload: one 4096 x 4096 scenario, Gaussian-random-field
 bathymetry with a shelf and ~10 % dry cells, four contiguous Okada
 subfaults, 3600 s simulated; seeded synthetic inputs (no dataset exists).
 
-A "step" is one time step of the whole grid (16.8 M cell-updates: the two
-stepping launches).  `value` = cell-updates/s over K steps with the state
+A "step" is one time step of the whole grid (16.8 M cell-updates: the five
+stepping launches - deep-water and general kernels of each phase and the
+step controller).  `value` = cell-updates/s over K steps with the state
 resident in HBM, timed with CUDA events on the stepping stream (the 268 MB
 state exceeds the 126 MB L2, so no flush is needed between steps).
 `e2e` = the same metric through the public C ABI (thy_run) on host
@@ -39,6 +40,7 @@ sys.path.insert(0, os.path.join(ROOT, "tsunami-hysea_b200"))
 METRIC = "cell-updates/s"
 BYTES_PHASE1 = 36   # eta, dep, qx, qy read (16) + eta written (4) + max-height/arrival/initial eta read, max written (16)
 BYTES_PHASE2 = 24   # eta, dep, qx, qy read (16) + qx, qy written (8)
+TILE_CELLS = 112 * 32   # cells of a full tile (kTileX x kTileY)
 
 
 def env_int(k, d):
@@ -230,20 +232,33 @@ def run_ours(a, dist: Dist):
     dev_s = dist.max(dev_ms / 1e3)
     total_cells = dist.sum(float(cells * a.steps))
     value = total_cells / dev_s
-    # per-kernel device time for the roofline (individually launched steps)
-    p1_ms, p2_ms = sess.profile(32)
+    # per-kernel device time for the roofline (individually launched steps);
+    # each kernel's algorithmic bytes count the cells it steps: deep tiles are
+    # interior tiles of TILE_CELLS cells, the general kernels step the rest
+    t0_tiles, t0_deep = sess.tiles()
+    prof_steps = 32
+    ms6 = sess.profile_launches(prof_steps)
+    t1_tiles, t1_deep = sess.tiles()
     sess.close()
+    deep_frac = (t1_deep - t0_deep) / max(1, t1_tiles - t0_tiles)
+    ntiles = (t1_tiles - t0_tiles) // prof_steps
+    cells_deep = (t1_deep - t0_deep) / prof_steps * TILE_CELLS
+    cells_gen = cells - cells_deep
     peak, peak_kind = measured_peak()
-    kern = {"phase1_mass_diag": (p1_ms, BYTES_PHASE1), "phase2_momentum_dt": (p2_ms, BYTES_PHASE2)}
+    kern = {"deep_phase1": (ms6[0], BYTES_PHASE1, cells_deep), "general_phase1": (ms6[1], BYTES_PHASE1, cells_gen),
+            "deep_phase2": (ms6[3], BYTES_PHASE2, cells_deep), "general_phase2": (ms6[4], BYTES_PHASE2, cells_gen)}
     dom = max(kern, key=lambda k: kern[k][0])
-    ms, bpc = kern[dom]
-    achieved = bpc * cells / (ms * 1e-3) / 1e9
+    ms, bpc, kcells = kern[dom]
+    achieved = bpc * kcells / (ms * 1e-3) / 1e9
     traffic = ncu_traffic(dom)
+    step_ms = sum(ms6)
     roofline = {"bound": "hbm", "kernel": dom, "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic, "peak_source": peak_kind,
-                "algorithmic_bytes_per_cell": bpc,
-                "per_kernel_ms": {k: round(v[0], 5) for k, v in kern.items()},
-                "step_frac_of_peak": round((BYTES_PHASE1 + BYTES_PHASE2) * cells / ((p1_ms + p2_ms) * 1e-3) / 1e9 / peak, 4)}
+                "algorithmic_bytes_per_cell": bpc, "cells_per_launch": int(kcells),
+                "per_kernel_ms": {**{k: round(v[0], 5) for k, v in kern.items()}, "classify": round(ms6[2], 5),
+                                  "controller": round(ms6[5], 5)},
+                "deep_tile_fraction": round(deep_frac, 4), "tiles": int(ntiles),
+                "step_frac_of_peak": round((BYTES_PHASE1 + BYTES_PHASE2) * cells / (step_ms * 1e-3) / 1e9 / peak, 4)}
     # end to end through the public API on host buffers: full 3600 s runs
     e2e = None
     if not a.skip_e2e:

@@ -122,6 +122,8 @@ typedef struct thy_stats {
     double device_loop_ms;    /* device time of the stepping kernels (CUDA events) */
     long long kernel_launches;/* kernels launched by the time loop */
     int snapshots, series_samples;
+    long long tiles;          /* phase-2 tiles stepped (steps x tiles of the grid) */
+    long long deep_tiles;     /* ... of which by the deep-water kernels */
 } thy_stats;
 
 /* Library / device. */
@@ -192,7 +194,12 @@ int thy_session_fetch(thy_session *s, float *max_height, float *eta, float *ux, 
 /* average device time (ms) of the phase-1 (mass + diagnostics) and phase-2
  * (momentum + dt) launches over `steps` individually launched steps */
 int thy_session_profile(thy_session *s, long long steps, double *phase1_ms, double *phase2_ms);
+/* the same, per launch: ms_per_launch[6] = deep phase 1, general phase 1,
+   deep/general classification, deep phase 2, general phase 2, step controller */
+int thy_session_profile_launches(thy_session *s, long long steps, double *ms_per_launch);
 long long thy_session_launches(const thy_session *s);   /* stepping kernels launched so far */
+/* phase-2 tiles stepped so far, and how many of them by the deep-water kernels */
+int thy_session_tiles(const thy_session *s, long long *tiles, long long *deep_tiles);
 double thy_session_time(const thy_session *s);    /* simulated time (s) */
 void thy_session_close(thy_session *s);
 

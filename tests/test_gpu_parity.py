@@ -112,3 +112,30 @@ def test_okada_deformation_matches_oracle(gpu):
     d = np.abs(g["deformed_bathy"].astype(np.float64) - r["deformed_bathy"])
     # FP32 storage of the depth: about one float ulp of a 7 km depth (~0.5 mm)
     assert d.max() <= 2e-3
+
+
+@pytest.mark.parametrize("borders", [(1.0, 1.0, 1.0, 1.0), (1.0, -1.0, 2.0, 2.0)], ids=["open", "periodic"])
+def test_deep_and_coastal_tiles(gpu, borders):
+    """1024^2 shelf: interior open-ocean tiles take the deep-water kernels,
+    coastal, border and sponge tiles the general ones; one result"""
+    p = synth.single_large(n=1024, seed=5, sim_time=900.0, save_time=300.0)
+    p.name = "deep1024"
+    p.borders = borders
+    g, r, c = _both(gpu, p)
+    _assert_parity(c)
+    assert 0 < g["deep_tiles"] < g["tiles"]
+    assert g["deep_tiles"] > g["tiles"] // 2
+
+
+def test_deep_tiles_fault_mid_run(gpu):
+    """a second fault at t = 300 s deforms the state between two steps: the
+    tile depth minima are re-measured before any tile is stepped as deep"""
+    import dataclasses
+
+    p = synth.single_large(n=512, seed=6, sim_time=900.0, save_time=150.0)
+    p.name = "deep512_twofault"
+    f0 = p.faults[0]
+    p.faults = [f0, dataclasses.replace(p.faults[2], time=300.0, slip=6.0)]
+    g, r, c = _both(gpu, p)
+    _assert_parity(c)
+    assert g["deep_tiles"] > 0

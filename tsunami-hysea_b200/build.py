@@ -98,7 +98,7 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         objs = list(ex.map(lambda s: _compile(s, verbose), sources))
     so = os.path.join(LIB, "libthysea.so")
     if not os.path.exists(so) or any(os.path.getmtime(o) > os.path.getmtime(so) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", so, *objs, "-lcuda"]
+        cmd = [NVCC, *ARCH, "-shared", "-o", so, *objs]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")

@@ -45,7 +45,7 @@ struct RowMetrics {
 };
 
 // Mutable per-scenario control block; written by the host between graph
-// launches and by the last tile of each phase-2 launch.
+// launches and by the controller launch that ends each step.
 struct ScenarioCtl {
     double t;            // simulated time (dimensionless)
     double dt;           // time step of the next step
@@ -62,11 +62,26 @@ struct ScenarioCtl {
     int jumping;               // the reference's saltar_deformacion
     int nfaults;
     unsigned int dt_bits;      // atomicMin target (positive float bits)
-    unsigned int tiles_done;   // phase-2 tiles finished this step
+    unsigned int tiles_done;   // phase-0 tiles finished (initial dt)
     unsigned int errors;       // non-finite values seen
     int pad_;
     const double *fault_times; // nfaults fault times (s), sorted, device memory
+    unsigned long long tiles_deep;   // phase-2 tiles stepped by the deep-water kernels
 };
+
+// Opaque 128-byte TMA tensor map (CUtensorMap), 64-byte aligned in device memory.
+struct alignas(64) TmaMap {
+    unsigned long long opaque[16];
+};
+
+// tensor maps of a scenario: state planes boxed kStageW x kStageRows (the
+// staged window of a half tile), diagnostics boxed kTileX x kHalfRows
+enum : int {
+    kMapEta0 = 0, kMapEta1, kMapQx0, kMapQx1, kMapQy0, kMapQy1, kMapDep, kMapEtaMax, kMapArr, kMapEtaIni, kNumMaps
+};
+constexpr int kHalfRows = 16;                 // rows of a half tile
+constexpr int kStageW = 120;                  // staged columns: x0-4 .. x0+115 (16-byte aligned start)
+constexpr int kStageRows = kHalfRows + 2;     // staged rows: one above and one below the half tile
 
 struct ScenarioDev {
     int nx, ny, pitch;
@@ -83,6 +98,16 @@ struct ScenarioDev {
     float *eta_max;
     float *arr;
     float *eta_ini;
+    // per half tile (rows 0-15 / 16-31 of tile t at 2t / 2t+1): minimum water
+    // depth eta + dep over its cells, written by phase 1 for the state it
+    // produces (index parity^1); NaN = unknown
+    float *tile_hmin[2];
+    // TMA tensor maps of the field planes (kMap* order), null when the grid
+    // is too small to have deep tiles
+    const struct TmaMap *tmap;
+    // per row y (ny+1 entries): {cos, ilcos, area, dlon} (dlon of edge row y;
+    // the other three unused in entry ny)
+    const float4 *rowpack;
     RowMetrics row;
     ScenarioCtl *ctl;
 };
@@ -180,6 +205,98 @@ __device__ __forceinline__ bool all_deep(const Edge &e, float hpos)
 }
 
 // ---------------------------------------------------------------------------
+// Edges whose four stencil cells are all deeper than hpos and which lie at
+// least two cells from a boundary: the 2s blend weight is exactly 1, so the
+// flux is the 2s flux alone (the WAF part, the wet/dry tests and the limiter
+// drop out).  The general functions below and the deep-water kernels both
+// call these, so both paths produce the same numbers.
+// ---------------------------------------------------------------------------
+
+// x edge: F = q0 len, outflow-limited (src/GPU/Arista_kernel.cu:118-219, alfa = 1)
+__device__ __forceinline__ float mass_2s_x(float q0, float len, float h0, float h1, float dt, float a0, float a1)
+{
+    return limit_outflow(q0 * len, h0, h1, 1.f, 1.f, dt, a0, a1);
+}
+
+// y edge: F = len q0 cos0 (src/GPU/Arista_kernel.cu:674-778, alfa = 1)
+__device__ __forceinline__ float mass_2s_y(float q0, float len, float cos0, float cos1, float h0, float h1, float dt,
+                                           float a0, float a1)
+{
+    return limit_outflow(len * q0 * cos0, h0, h1, cos0, cos1, dt, a0, a1);
+}
+
+// Result of a momentum flux: contributions to the two cells (already with
+// the "acc -= F" sign applied) and the wave-speed term for the time step.
+struct MomFlux {
+    float m_x, m_y;   // to cell0: subtract
+    float p_x, p_y;   // to cell1: subtract
+    float lam;        // edge length * max wave speed (added to both)
+    bool active;
+};
+
+// Per-cell factors of the 2s fluxes, computed once per cell and shared by
+// its four edges: 1/h (approximate reciprocal) and sqrt(h).
+__device__ __forceinline__ float rcp_depth(float h) { return __fdividef(1.f, h); }
+
+// x edge, components (qx, qy); u = qx normal, v = qy tangential, rh = 1/h,
+// sh = sqrt(h) of each side, jump = the surface jump, asum = area0 + area1
+// (src/GPU/Arista_kernel.cu:221-464, alfa = 1)
+__device__ __forceinline__ void momentum_2s_x(MomFlux &r, float h0, float h1, float rh0, float rh1, float s0, float s1,
+                                              float u0, float u1, float v0, float v1, float jump, float ilcos,
+                                              float asum, float dt, float cvis)
+{
+    const float hij = 0.5f * (h0 + h1);
+    const float u0n = u0 * rh0, u1n = u1 * rh1;
+    const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
+    const float maxa = fabsf(uijn) + sqrtf(hij);
+    float mx, my, px, py;
+    if (uijn < 0.f) {
+        mx = u1n * u1 * ilcos; px = -mx; mx += hij * jump * ilcos;
+        my = u1n * v1 * ilcos; py = -my;
+    } else {
+        mx = u0n * u0 * ilcos; px = -mx; mx += hij * jump * ilcos;
+        my = u0n * v0 * ilcos; py = -my;
+    }
+    const float cd = 0.5f * (1.f - cvis);
+    const float val = (2.f * ilcos * dt) / asum;
+    const float des = cd * val * maxa * maxa * (u1 - u0) * ilcos;
+    r.m_x = mx - des; r.m_y = my;
+    r.p_x = px + des; r.p_y = py;
+    r.lam = ilcos * maxa;
+    r.active = true;
+}
+
+// y edge, components (qx, qy); u = qy normal, v = qx tangential; icos =
+// 1/cos(lat) of each side's row, correctly rounded
+// (src/GPU/Arista_kernel.cu:780-1026, alfa = 1)
+__device__ __forceinline__ void momentum_2s_y(MomFlux &r, float h0, float h1, float rh0, float rh1, float s0, float s1,
+                                              float u0, float u1, float v0, float v1, float jump, float cos0,
+                                              float cos1, float icos0, float icos1, float len, float asum, float dt,
+                                              float cvis)
+{
+    const float hij = 0.5f * (h0 + h1);
+    const float u0n = u0 * rh0, u1n = u1 * rh1;
+    const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
+    const float maxa = fabsf(uijn) + sqrtf(hij);
+    const float deta = 0.5f * (cos0 + cos1) * jump - uijn * uijn * (cos1 - cos0);
+    float fym, fyp, fxm, fxp;
+    if (uijn < 0.f) {
+        fym = u1n * u1 * len; fyp = -fym; fym *= cos1 * icos0; fym += hij * deta * len * icos0;
+        fxm = u1n * v1 * len; fxp = -fxm;
+    } else {
+        fym = u0n * u0 * len; fyp = -fym * cos0 * icos1; fym += hij * deta * len * icos0;
+        fxm = u0n * v0 * len; fxp = -fxm;
+    }
+    const float val = (2.f * len * dt) / asum;
+    const float cd = 0.5f * (1.f - cvis);
+    const float des = cd * val * maxa * maxa * (u1 * cos1 - u0 * cos0) * len;
+    r.m_x = fxm; r.m_y = fym - des * icos0;
+    r.p_x = fxp; r.p_y = fyp + des * icos1;
+    r.lam = len * maxa;
+    r.active = true;
+}
+
+// ---------------------------------------------------------------------------
 // phase 1: mass flux through one edge (src/GPU/Arista_kernel.cu:118-219 for
 // x edges, 674-778 for y edges).  Returns F; the caller applies it as
 // cell0 -= F (/cos0 for y), cell1 += F (/cos1).
@@ -188,8 +305,8 @@ template <bool LAT>
 __device__ __forceinline__ float mass_flux(Edge &e, const ScenarioDev &s, float dt)
 {
     if (all_deep(e, s.hpos)) {
-        if (!LAT) return limit_outflow(e.u0 * e.len, e.h0, e.h1, 1.f, 1.f, dt, e.area0, e.area1);
-        return limit_outflow(e.len * e.u0 * e.cos0, e.h0, e.h1, e.cos0, e.cos1, dt, e.area0, e.area1);
+        if (!LAT) return mass_2s_x(e.u0, e.len, e.h0, e.h1, dt, e.area0, e.area1);
+        return mass_2s_y(e.u0, e.len, e.cos0, e.cos1, e.h0, e.h1, dt, e.area0, e.area1);
     }
     if (e.front) swap_sides(e);
     const float h0 = e.h0, h1 = e.h1;
@@ -237,15 +354,6 @@ __device__ __forceinline__ float mass_flux(Edge &e, const ScenarioDev &s, float 
     return limit_outflow(F, h0, h1, e.cos0, e.cos1, dt, e.area0, e.area1);
 }
 
-// Result of a momentum flux: contributions to the two cells (already with
-// the "acc -= F" sign applied) and the wave-speed term for the time step.
-struct MomFlux {
-    float m_x, m_y;   // to cell0: subtract
-    float p_x, p_y;   // to cell1: subtract
-    float lam;        // edge length * max wave speed (added to both)
-    bool active;
-};
-
 // ---------------------------------------------------------------------------
 // phase 2: momentum flux of an x edge (src/GPU/Arista_kernel.cu:221-464).
 // Components are (qx, qy).
@@ -256,26 +364,8 @@ __device__ __forceinline__ MomFlux momentum_flux_x(Edge &e, const ScenarioDev &s
     r.active = true;
     const float ilcos = e.len;
     if (all_deep(e, s.hpos)) {
-        const float h0 = e.h0, h1 = e.h1, hij = 0.5f * (h0 + h1);
-        const float u0n = __fdividef(e.u0, h0), u1n = __fdividef(e.u1, h1);
-        const float s0 = sqrtf(h0), s1 = sqrtf(h1);
-        const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
-        const float maxa = fabsf(uijn) + sqrtf(hij);
-        const float jump = surface_jump(e.e0, e.e1, e.D0, e.D1);
-        float mx, my, px, py;
-        if (uijn < 0.f) {
-            mx = u1n * e.u1 * ilcos; px = -mx; mx += hij * jump * ilcos;
-            my = u1n * e.v1 * ilcos; py = -my;
-        } else {
-            mx = u0n * e.u0 * ilcos; px = -mx; mx += hij * jump * ilcos;
-            my = u0n * e.v0 * ilcos; py = -my;
-        }
-        const float cd = 0.5f * (1.f - s.cvis);
-        const float val = (2.f * ilcos * dt) / (e.area0 + e.area1);
-        const float des = cd * val * maxa * maxa * (e.u1 - e.u0) * ilcos;
-        r.m_x = mx - des; r.m_y = my;
-        r.p_x = px + des; r.p_y = py;
-        r.lam = ilcos * maxa;
+        momentum_2s_x(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrtf(e.h0), sqrtf(e.h1), e.u0, e.u1, e.v0,
+                      e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1), ilcos, e.area0 + e.area1, dt, s.cvis);
         return r;
     }
     if (e.front) swap_sides(e);
@@ -365,28 +455,9 @@ __device__ __forceinline__ MomFlux momentum_flux_y(Edge &e, const ScenarioDev &s
     r.active = true;
     const float len = e.len;
     if (all_deep(e, s.hpos)) {
-        const float icos0 = __frcp_rn(e.cos0), icos1 = __frcp_rn(e.cos1);
-        const float h0 = e.h0, h1 = e.h1, hij = 0.5f * (h0 + h1);
-        const float u0n = __fdividef(e.u0, h0), u1n = __fdividef(e.u1, h1);
-        const float s0 = sqrtf(h0), s1 = sqrtf(h1);
-        const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
-        const float maxa = fabsf(uijn) + sqrtf(hij);
-        const float deta = 0.5f * (e.cos0 + e.cos1) * surface_jump(e.e0, e.e1, e.D0, e.D1) -
-                           uijn * uijn * (e.cos1 - e.cos0);
-        float fym, fyp, fxm, fxp;
-        if (uijn < 0.f) {
-            fym = u1n * e.u1 * len; fyp = -fym; fym *= e.cos1 * icos0; fym += hij * deta * len * icos0;
-            fxm = u1n * e.v1 * len; fxp = -fxm;
-        } else {
-            fym = u0n * e.u0 * len; fyp = -fym * e.cos0 * icos1; fym += hij * deta * len * icos0;
-            fxm = u0n * e.v0 * len; fxp = -fxm;
-        }
-        const float val = (2.f * len * dt) / (e.area0 + e.area1);
-        const float cd = 0.5f * (1.f - s.cvis);
-        const float des = cd * val * maxa * maxa * (e.u1 * e.cos1 - e.u0 * e.cos0) * len;
-        r.m_x = fxm; r.m_y = fym - des * icos0;
-        r.p_x = fxp; r.p_y = fyp + des * icos1;
-        r.lam = len * maxa;
+        momentum_2s_y(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrtf(e.h0), sqrtf(e.h1), e.u0, e.u1, e.v0,
+                      e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1), e.cos0, e.cos1, __frcp_rn(e.cos0),
+                      __frcp_rn(e.cos1), len, e.area0 + e.area1, dt, s.cvis);
         return r;
     }
     if (e.front) swap_sides(e);

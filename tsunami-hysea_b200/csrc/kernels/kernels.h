@@ -13,11 +13,30 @@ constexpr int kTileX = 28 * (kStepThreads / 32);   // tile width: 28 output colu
 constexpr int kTileY = 32;                  // tile height: rows one warp marches through
 
 // step.cu
-size_t step_smem_bytes();
 cudaError_t configure_step_kernels();
 int step_blocks_per_sm();
-// phase 0: initial dt; 1: mass + diagnostics; 2: momentum + dt + controller
-void launch_step_phase(int phase, const ScenarioDev *scen, const int2 *work, const int *nwork, int grid, cudaStream_t st);
+// Launch parameters of the stepping kernels of a batch.
+struct StepLaunch {
+    const ScenarioDev *scen;   // scenario table (nslots entries)
+    const int2 *work;          // work list: (scenario slot, tile)
+    const int *nwork;          // its length (device)
+    int *lists;                // deep / general lists of the step: 2 counts + 2 x cap indices
+    int cap;                   // list capacity (>= work-list length)
+    int grid;                  // general kernel grid
+    int deep_grid[2];          // persistent deep kernel grids, phase 1 and 2
+    int classify_grid;
+    int nslots;
+};
+
+// The kLaunchesPerStep launches of a time step, in order: 0 deep phase 1,
+// 1 general phase 1, 2 work-list classification, 3 deep phase 2, 4 general
+// phase 2, 5 step controller.  Launches 0/1 and 3/4 may run concurrently.
+constexpr int kLaunchesPerStep = 6;
+void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st);
+void launch_initial_dt(const StepLaunch &L, cudaStream_t st);
+// every work item on the general list (after the host changed a state)
+void launch_lists_all_general(const StepLaunch &L, cudaStream_t st);
+int deep_blocks_per_sm(int phase);
 
 // init.cu: double-precision host state (reference layout, dimensionless) to
 // the FP32 device state; metrics initialised as in src/GPU/ShallowWater.cu:305-309

@@ -1,14 +1,23 @@
 // Time-step kernels of the B200 stepper.
 //
-// One time step = two launches over a work list of (scenario, tile) items:
+// One time step = five launches over a work list of (scenario, tile) items:
 //   phase 1  mass fluxes -> new surface elevation, fused with the
 //            max-height / arrival-time diagnostics of the state the step
-//            starts from (src/GPU/Metrics.cu:23-77);
+//            starts from (src/GPU/Metrics.cu:23-77) and with the minimum
+//            water depth of each tile of the new state;
 //   phase 2  momentum fluxes with the phase-1 depths -> new discharges,
 //            sponge, shallow-water filter, Manning friction, local CFL dt,
-//            tile min -> one atomicMin per tile; the last tile of a
-//            scenario runs the step controller (time, next dt, events).
-// Phase 0 (same template) computes the initial dt.
+//            tile min -> one atomicMin per tile;
+//   control  one thread per scenario: time, next dt, events.
+// Phases 1 and 2 are each a deep-water kernel and a general kernel.  A tile
+// is deep when every cell within two cells of it is deeper than hpos and it
+// is at least two cells from the boundaries and outside the sponge layers:
+// then every edge flux is the pure 2s flux and no cell is dried, damped or
+// relaxed, and the deep kernel marches the tile with a two-row window and
+// a fraction of the instructions and registers.  Both kernels evaluate the
+// same predicate on per-tile minimum depths that no launch of the phase
+// writes, so every tile is stepped by exactly one of them.
+// Phase 0 (the general template) computes the initial dt.
 //
 // Row marching: a tile is kWarps column strips side by side; in a strip each
 // lane owns one column and the warp marches down the tile's rows keeping a
@@ -71,20 +80,39 @@ __device__ __forceinline__ Cell load_cell(const float *__restrict__ eta, const f
     return c;
 }
 
-// raw loads of a row that is still in flight (prefetch two rows ahead)
+// raw loads of a row that is still in flight (prefetch two rows ahead); in
+// phase 1 also the cell's max-height / arrival-time / initial-surface values
 struct RawCell {
     float e, D, qx, qy;
+    float em, ar, ei;
 };
 
-__device__ __forceinline__ RawCell load_raw(const float *__restrict__ eta, const float *__restrict__ dep,
-                                            const float *__restrict__ qx, const float *__restrict__ qy, size_t idx)
+template <bool DIAG>
+__device__ __forceinline__ RawCell load_raw(const ScenarioDev &s, const float *__restrict__ eta,
+                                            const float *__restrict__ qx, const float *__restrict__ qy, size_t idx,
+                                            bool diag)
 {
     RawCell r;
     r.e = __ldg(eta + idx);
-    r.D = __ldg(dep + idx);
+    r.D = __ldg(s.dep + idx);
     r.qx = __ldg(qx + idx);
     r.qy = __ldg(qy + idx);
+    r.em = r.ar = r.ei = 0.f;
+    if (DIAG && diag) {
+        r.em = s.eta_max[idx];
+        r.ar = s.arr[idx];
+        r.ei = __ldg(s.eta_ini + idx);
+    }
     return r;
+}
+
+// Max-height / arrival-time update of one cell from the state the step starts
+// from (src/GPU/Metrics.cu:23-77).
+__device__ __forceinline__ void diagnostics(const ScenarioDev &s, const RawCell &r, size_t idx, float t_sec)
+{
+    const float h = r.e + r.D;
+    if (r.e > r.em && h > s.eps_h) s.eta_max[idx] = r.e;
+    if (r.ar < 0.f && fabsf(r.e - r.ei) > s.dif_at) s.arr[idx] = t_sec;
 }
 
 __device__ __forceinline__ Cell finish(const RawCell &r)
@@ -119,7 +147,7 @@ __device__ __forceinline__ float initial_speed(Edge &e, const ScenarioDev &s)
     return e.len * maxa;
 }
 
-// Step controller, run by the last phase-2 tile of a scenario
+// Step controller of one scenario, run after its phase-2 tiles
 // (src/GPU/ShallowWater.cu:397-450 loop body after the step;
 //  src/GPU/Timestep.cu:35-68 dt truncation to fault times).
 __device__ void controller(const ScenarioDev &s)
@@ -232,15 +260,444 @@ __device__ __forceinline__ void y_edge(const ScenarioDev &s, const Cell &m, cons
     }
 }
 
+// Deep-tile predicate; hmin = half-tile minimum depths of the state the phase
+// reads.  The geometric tests imply 1 <= tx <= tiles_x - 2 and
+// 1 <= ty <= tiles_y - 2; the stencil reaches two cells beyond the tile, so
+// the lower half of the tile row above, both halves of the tile's own row and
+// the upper half of the row below are checked, for the tile and its left and
+// right neighbours.  Unknown minima are NaN and fail the comparison.
+__device__ __forceinline__ bool tile_is_deep(const ScenarioDev &s, const float *__restrict__ hmin, int tx, int ty)
+{
+    if (!s.tmap) return false;
+    const int x0 = tx * kTileX, y0 = ty * TY;
+    if (x0 < max(2, s.sp_left) || x0 + kTileX > s.nx - max(2, s.sp_right)) return false;
+    if (y0 < max(2, s.sp_up) || y0 + TY > s.ny - max(2, s.sp_low)) return false;
+    const float *up = hmin + 2 * ((size_t)(ty - 1) * s.tiles_x + (tx - 1));
+    const float *mid = up + 2 * s.tiles_x, *dn = mid + 2 * s.tiles_x;
+    const float hp = s.hpos;
+    bool ok = true;
+    for (int k = 0; k < 3; k++)
+        ok = ok && (up[2 * k + 1] > hp) && (mid[2 * k] > hp) && (mid[2 * k + 1] > hp) && (dn[2 * k] > hp);
+    return ok;
+}
+
+// ---------------------------------------------------------------------------
+// TMA staging: one elected thread issues 2D tensor copies of a half tile's
+// window into shared memory, completing on an mbarrier that every thread
+// waits on with an iteration limit.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// at most 2^20 polls (each try_wait may suspend the thread for a while)
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
+{
+    for (int i = 0; i < (1 << 20); i++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+// 2D tile load; x must be a multiple of 4 floats (16 bytes)
+__device__ __forceinline__ void tma_load_2d(float *dst, const TmaMap *map, int x, int y, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+        ::"r"(smem_addr(dst)), "l"(map), "r"(x), "r"(y), "r"(smem_addr(bar))
+        : "memory");
+}
+
+__device__ __forceinline__ void tmap_acquire(const TmaMap *map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
+}
+
+constexpr int DWARPS = 8;                           // 4 column strips x 2 row groups
+constexpr int DNT = DWARPS * 32;
+constexpr int DROWS = kHalfRows / 2;                // rows a warp marches
+constexpr int SPLANE = (kStageRows * kStageW + 31) / 32 * 32;   // floats per staged plane (128-byte multiple)
+constexpr int DPLANE = kHalfRows * kTileX;          // floats per staged diagnostics plane
+constexpr uint32_t kStateBytes = kStageRows * kStageW * 4;
+constexpr uint32_t kDiagBytes = kHalfRows * kTileX * 4;
+static_assert(kTileX % 4 == 0, "TMA x coordinates x0 - 4 and x0 must be 16-byte aligned");
+static_assert(kTileY == 2 * kHalfRows, "two half tiles per tile");
+static_assert((SPLANE * 4) % 128 == 0 && (DPLANE * 4) % 128 == 0, "staged planes 128-byte aligned");
+
+// Shared memory of a deep kernel CTA: two staging buffers (double buffering
+// across work units), then the two mbarriers, the staged row metrics of the
+// current unit and the reduction scratch.
+__host__ __device__ constexpr size_t deep_stage_bytes(int phase)
+{
+    return (size_t)(4 * SPLANE + (phase == 1 ? 3 * DPLANE : 0)) * sizeof(float);
+}
+struct DeepRow {
+    float4 m;      // cos, ilcos, area, dlon (edge row)
+    float icos;    // 1/cos, correctly rounded
+    float pad[3];
+};
+__host__ __device__ constexpr size_t deep_misc_offset(int phase) { return 2 * deep_stage_bytes(phase); }
+static size_t deep_smem_bytes(int phase)
+{
+    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + DWARPS * sizeof(float);
+}
+
+// one cell of a staged row (shared memory; the depth is formed here)
+__device__ __forceinline__ Cell staged_cell(const float *st, int i)
+{
+    Cell c;
+    c.e = st[i];
+    c.D = st[SPLANE + i];
+    c.qx = st[2 * SPLANE + i];
+    c.qy = st[3 * SPLANE + i];
+    c.h = c.e + c.D;
+    return c;
+}
+
+// Work lists of a step (device memory, cap entries each): lists[0] = deep
+// count, lists[1] = general count, deep work-list indices at lists + 2,
+// general ones at lists + 2 + cap.
+__device__ __forceinline__ const int *deep_items(const int *lists) { return lists + 2; }
+__device__ __forceinline__ const int *general_items(const int *lists, int cap) { return lists + 2 + cap; }
+
+// Splits the work list into deep and general items for the state the next
+// phase reads: after phase 1 of a running scenario that is the state phase 1
+// produced (minima at parity^1), which phase 2 of this step and phase 1 of the
+// next step both read; for a scenario that is not running it is the state at
+// its current parity.  all_general (after any change of the state by the
+// host) puts every item on the general list.  The counts are zeroed before.
+__global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+                                const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int all_general)
+{
+    const int n = *nwork_ptr;
+    const int lane = threadIdx.x & 31;
+    for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
+        const int w = base + threadIdx.x;
+        bool deep = false;
+        if (w < n && !all_general) {
+            const int2 item = work[w];
+            const ScenarioDev &s = scen[item.x];
+            const ScenarioCtl *ctl = s.ctl;
+            const int p = ctl->parity;
+            const int par = (ctl->status == kRunning) ? (p ^ 1) : p;
+            const int ty = item.y / s.tiles_x, tx = item.y - ty * s.tiles_x;
+            deep = tile_is_deep(s, s.tile_hmin[par], tx, ty);
+        }
+        // warp-aggregated appends
+        const unsigned in_range = __ballot_sync(0xffffffffu, w < n);
+        const unsigned dm = __ballot_sync(0xffffffffu, deep && w < n);
+        const unsigned gm = in_range & ~dm;
+        int dbase = 0, gbase = 0;
+        if (lane == 0) {
+            if (dm) dbase = atomicAdd(&lists[0], __popc(dm));
+            if (gm) gbase = atomicAdd(&lists[1], __popc(gm));
+        }
+        dbase = __shfl_sync(0xffffffffu, dbase, 0);
+        gbase = __shfl_sync(0xffffffffu, gbase, 0);
+        const unsigned below = (1u << lane) - 1u;
+        if (w < n) {
+            if (deep) lists[2 + dbase + __popc(dm & below)] = w;
+            else lists[2 + cap + gbase + __popc(gm & below)] = w;
+        }
+    }
+}
+
+// y edge between rows gy-1 (a, row metrics ra) and gy (b, rb) of a deep tile;
+// phase 2 also takes 1/h and sqrt(h) of both cells
+template <int PHASE>
+__device__ __forceinline__ void y_edge_deep(const ScenarioDev &s, const Cell &a, const Cell &b, float rha, float sha,
+                                            float rhb, float shb, const DeepRow &ra, const DeepRow &rb, float dt,
+                                            Contrib &lo, Contrib &hi)
+{
+    const float cos0 = ra.m.x, cos1 = rb.m.x, area0 = ra.m.z, area1 = rb.m.z, len = rb.m.w;
+    if (PHASE == 1) {
+        const float F = mass_2s_y(a.qy, len, cos0, cos1, a.h, b.h, dt, area0, area1);
+        lo = {-F / cos0, 0.f, 0.f};
+        hi = {F / cos1, 0.f, 0.f};
+    } else {
+        MomFlux f;
+        momentum_2s_y(f, a.h, b.h, rha, rhb, sha, shb, a.qy, b.qy, a.qx, b.qx, surface_jump(a.e, b.e, a.D, b.D), cos0,
+                      cos1, ra.icos, rb.icos, len, area0 + area1, dt, s.cvis);
+        lo = {-f.m_x, -f.m_y, f.lam};
+        hi = {-f.p_x, -f.p_y, f.lam};
+    }
+}
+
+// A deep work unit: half `half` of work item `w`.
+struct DeepUnit {
+    const ScenarioDev *s;
+    int tile, half, x0, yb, p;
+    bool run;
+};
+
+__device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+                                              const int *__restrict__ lists, int u)
+{
+    DeepUnit d;
+    const int2 item = work[deep_items(lists)[u >> 1]];
+    d.s = &scen[item.x];
+    d.tile = item.y;
+    d.half = u & 1;
+    const int ty = item.y / d.s->tiles_x, tx = item.y - ty * d.s->tiles_x;
+    d.x0 = tx * kTileX;
+    d.yb = ty * TY + d.half * kHalfRows;
+    const ScenarioCtl *ctl = d.s->ctl;
+    d.p = ctl->parity;
+    d.run = *((volatile const int *)&ctl->status) == kRunning;
+    return d;
+}
+
+// TMA copies of a unit's window into one staging buffer (one thread).  The
+// maps are written by host copies before the launch; a CTA acquires a
+// scenario's maps once, when it first copies from that scenario (acq).
+template <int PHASE>
+__device__ __forceinline__ void deep_issue(const DeepUnit &d, float *stage, uint64_t *bar, const TmaMap *&acq)
+{
+    const TmaMap *m = d.s->tmap;
+    const int p = d.p;
+    const int me = (PHASE == 2) ? kMapEta0 + (p ^ 1) : kMapEta0 + p;
+    if (m != acq) {
+        for (int k = 0; k < kNumMaps; k++) tmap_acquire(m + k);
+        acq = m;
+    }
+    mbar_expect_tx(bar, 4 * kStateBytes + (PHASE == 1 ? 3 * kDiagBytes : 0));
+    tma_load_2d(stage, m + me, d.x0 - 4, d.yb - 1, bar);
+    tma_load_2d(stage + SPLANE, m + kMapDep, d.x0 - 4, d.yb - 1, bar);
+    tma_load_2d(stage + 2 * SPLANE, m + kMapQx0 + p, d.x0 - 4, d.yb - 1, bar);
+    tma_load_2d(stage + 3 * SPLANE, m + kMapQy0 + p, d.x0 - 4, d.yb - 1, bar);
+    if (PHASE == 1) {
+        tma_load_2d(stage + 4 * SPLANE, m + kMapEtaMax, d.x0, d.yb, bar);
+        tma_load_2d(stage + 4 * SPLANE + DPLANE, m + kMapArr, d.x0, d.yb, bar);
+        tma_load_2d(stage + 4 * SPLANE + 2 * DPLANE, m + kMapEtaIni, d.x0, d.yb, bar);
+    }
+}
+
+// Phase 1 / 2 of the deep tiles, persistent: CTA b steps units b, b + grid,
+// ... of the deep list (two per tile: its upper and lower half).  A unit's
+// window - its rows plus one above and one below, columns x0-4 .. x0+115 of
+// eta, dep, qx, qy, and in phase 1 the diagnostics of its own cells - is
+// staged by TMA, the next unit's copy in flight while the current one is
+// computed.  Warp w marches rows 8 (w >> 2) .. +7 of column strip w & 3 (28
+// output columns, lanes 2..29) with a two-row window.
+template <int PHASE>
+__global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+                                                   const int *__restrict__ lists)
+{
+    extern __shared__ __align__(1024) unsigned char dsm[];
+    constexpr size_t SB = deep_stage_bytes(PHASE);
+    // staging buffer b at dsm + b * SB
+    uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + deep_misc_offset(PHASE));
+    DeepRow *rows = reinterpret_cast<DeepRow *>(dsm + deep_misc_offset(PHASE) + 16);
+    float *red = reinterpret_cast<float *>(rows + kStageRows);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int strip = warp & 3, group = warp >> 2;
+    const int nunits = 2 * lists[0];
+    if (blockIdx.x >= nunits) return;
+    // TMA destinations must be 128-byte aligned: a misaligned buffer is
+    // reported on every scenario of the CTA's units and nothing is copied
+    if (smem_addr(dsm) & 127u) {
+        if (threadIdx.x == 0)
+            for (int u = blockIdx.x; u < nunits; u += gridDim.x)
+                atomicOr(&scen[work[deep_items(lists)[u >> 1]].x].ctl->errors, 4u);
+        return;
+    }
+    if (threadIdx.x == 0) {
+        mbar_init(&bars[0]);
+        mbar_init(&bars[1]);
+    }
+    __syncthreads();
+    uint32_t phase_bits = 0;     // bit b: parity of the next completion of bars[b]
+    const TmaMap *acq = nullptr; // maps acquired by this CTA (thread 0)
+    DeepUnit d = deep_unit(scen, work, lists, blockIdx.x);
+    if (threadIdx.x == 0 && d.run) deep_issue<PHASE>(d, reinterpret_cast<float *>(dsm), &bars[0], acq);
+    int buf = 0;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x, buf ^= 1) {
+        // the next unit's copy goes to the other buffer, free since the end of the previous unit
+        const int un = u + gridDim.x;
+        DeepUnit dn;
+        dn.run = false;
+        if (un < nunits) {
+            dn = deep_unit(scen, work, lists, un);
+            if (threadIdx.x == 0 && dn.run)
+                deep_issue<PHASE>(dn, reinterpret_cast<float *>(dsm + (buf ^ 1) * SB), &bars[buf ^ 1], acq);
+        }
+        const ScenarioDev &s = *d.s;
+        ScenarioCtl *ctl = s.ctl;
+        const int x0 = d.x0, yb = d.yb, p = d.p;
+        if (d.run) {
+            // row metrics of the window while the copies are in flight
+            if (threadIdx.x < kStageRows) {
+                DeepRow r;
+                r.m = __ldg(s.rowpack + yb - 1 + threadIdx.x);
+                r.icos = __frcp_rn(r.m.x);
+                rows[threadIdx.x] = r;
+            }
+            const bool ok = mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u);
+            phase_bits ^= 1u << buf;
+            if (__syncthreads_or(!ok)) {
+                // the copies did not land in time: report, give both buffers'
+                // copies one more bounded wait so none is still writing, stop
+                if (threadIdx.x == 0) atomicOr(&ctl->errors, 2u);
+                mbar_wait_bounded(&bars[buf], ((phase_bits >> buf) & 1u) ^ 1u);
+                if (dn.run) mbar_wait_bounded(&bars[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u);
+                return;
+            }
+            const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
+            const float dt = (float)ctl->dt;
+            const float t_sec = (float)(ctl->t * ctl->T);
+            const int pitch = s.pitch;
+            const int r_first = group * DROWS + 1;                  // staged row of this warp's first output row
+            const int sc = strip * 28 + 2 + lane;                   // staged column of this lane
+            const int gx = x0 - 4 + sc;                             // grid column
+            const bool has_cell = (lane >= 2) && (lane <= 29);
+            const int dcol = strip * 28 - 2 + lane;                 // diagnostics column (cells only)
+            float local_min = FLT_MAX;
+            bool bad = false;
+            int i = r_first * kStageW + sc;
+            Cell c = staged_cell(stage, i);
+            float rh_c = 0.f, sh_c = 0.f;
+            if (PHASE == 2) {
+                rh_c = rcp_depth(c.h);
+                sh_c = sqrtf(c.h);
+            }
+            DeepRow rc = rows[r_first];
+            Contrib top;
+            {
+                const Cell a = staged_cell(stage, i - kStageW);
+                float rh_a = 0.f, sh_a = 0.f;
+                if (PHASE == 2) {
+                    rh_a = rcp_depth(a.h);
+                    sh_a = sqrtf(a.h);
+                }
+                Contrib dummy;
+                y_edge_deep<PHASE>(s, a, c, rh_a, sh_a, rh_c, sh_c, rows[r_first - 1], rc, dt, dummy, top);
+            }
+            float *out0 = (PHASE == 1) ? s.eta[p ^ 1] : s.qx[p ^ 1];
+            float *out1 = s.qy[p ^ 1];
+            int off = (yb + r_first - 1) * pitch + gx;
+            for (int k = 0; k < DROWS; k++, i += kStageW, off += pitch) {
+                const DeepRow rn = rows[r_first + k + 1];
+                const Cell n = staged_cell(stage, i + kStageW);
+                const float area = rc.m.z;
+                float rh_n = 0.f, sh_n = 0.f;
+                if (PHASE == 2) {
+                    rh_n = rcp_depth(n.h);
+                    sh_n = sqrtf(n.h);
+                }
+                // y edge below this row
+                Contrib below, next_top;
+                y_edge_deep<PHASE>(s, c, n, rh_c, sh_c, rh_n, sh_n, rc, rn, dt, below, next_top);
+                // x edge left of this lane's cell
+                Contrib xl, xr;
+                if (PHASE == 1) {
+                    const float F = mass_2s_x(stage[2 * SPLANE + i - 1], rc.m.y, stage[i - 1] + stage[SPLANE + i - 1],
+                                              c.h, dt, area, area);
+                    xl = {-F, 0.f, 0.f};
+                    xr = {F, 0.f, 0.f};
+                } else {
+                    const float e0 = stage[i - 1], D0 = stage[SPLANE + i - 1];
+                    MomFlux f;
+                    momentum_2s_x(f, e0 + D0, c.h, shup(rh_c, 1), rh_c, shup(sh_c, 1), sh_c, stage[2 * SPLANE + i - 1],
+                                  c.qx, stage[3 * SPLANE + i - 1], c.qy, surface_jump(e0, c.e, D0, c.D), rc.m.y,
+                                  area + area, dt, s.cvis);
+                    xl = {-f.m_x, -f.m_y, f.lam};
+                    xr = {-f.p_x, -f.p_y, f.lam};
+                }
+                // the right edge of this cell is the left edge of lane+1
+                Contrib xrr;
+                xrr.a = shdn(xl.a, 1);
+                if (PHASE == 2) {
+                    xrr.b = shdn(xl.b, 1);
+                    xrr.lam = shdn(xl.lam, 1);
+                }
+                if (has_cell) {
+                    if (PHASE == 1) {
+                        // diagnostics of the state the step starts from (src/GPU/Metrics.cu:23-77)
+                        const float *dg = stage + 4 * SPLANE + (r_first - 1 + k) * kTileX + dcol;
+                        const float em = dg[0], ar = dg[DPLANE], ei = dg[2 * DPLANE];
+                        if (c.e > em && c.h > s.eps_h) s.eta_max[off] = c.e;
+                        if (ar < 0.f && fabsf(c.e - ei) > s.dif_at) s.arr[off] = t_sec;
+                        // mass update (src/GPU/Volumen_kernel.cu:111-157)
+                        const float acc = ((xr.a + xrr.a) + top.a) + below.a;
+                        float eta = c.e + __fdividef(dt, area) * acc;
+                        if (!(eta + c.D > 0.f)) eta = -c.D;
+                        if (!isfinite(eta)) bad = true;
+                        out0[off] = eta;
+                        local_min = fminf(local_min, eta + c.D);
+                    } else {
+                        // momentum update; no sponge, filter or friction in a deep tile
+                        const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
+                        const float step = (lam < kEps) ? 1e30f : __fdividef(2.f * s.cfl * area, lam);
+                        local_min = fminf(local_min, step);
+                        const float val = __fdividef(dt, area);
+                        const float qx = c.qx + val * (((xr.a + xrr.a) + top.a) + below.a);
+                        const float qy = c.qy + val * (((xr.b + xrr.b) + top.b) + below.b);
+                        if (!isfinite(qx) || !isfinite(qy)) bad = true;
+                        out0[off] = qx;
+                        out1[off] = qy;
+                    }
+                }
+                top = next_top;
+                rc = rn;
+                c = n;
+                rh_c = rh_n;
+                sh_c = sh_n;
+            }
+            if (bad) atomicOr(&ctl->errors, 1u);
+            for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+            if (lane == 0) red[warp] = local_min;
+        }
+        __syncthreads();   // every warp is done with the staged window and the row metrics
+        if (d.run && threadIdx.x == 0) {
+            float m = red[0];
+            for (int k = 1; k < DWARPS; k++) m = fminf(m, red[k]);
+            if (PHASE == 1) {
+                s.tile_hmin[p ^ 1][2 * d.tile + d.half] = m;
+            } else {
+                atomicMin(&ctl->dt_bits, __float_as_uint(m));
+                if (d.half == 0) atomicAdd(&ctl->tiles_deep, 1ull);
+            }
+        }
+        __syncthreads();   // red[] is reused by the next unit
+        d = dn;
+    }
+}
+
+// General kernel: phase 0 over the whole work list, phases 1 and 2 over the
+// general list of the step.
 template <int PHASE>
 __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                                  const int *__restrict__ nwork_ptr)
+                                                  const int *__restrict__ nwork_ptr, const int *__restrict__ lists,
+                                                  int cap)
 {
-    __shared__ float red[WARPS];
-    __shared__ int is_last;
+    __shared__ float red[2 * WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nwork = *nwork_ptr;
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const int nitems = (PHASE == 0) ? *nwork_ptr : lists[1];
+    for (int g = blockIdx.x; g < nitems; g += gridDim.x) {
+        const int w = (PHASE == 0) ? g : general_items(lists, cap)[g];
         const int2 item = work[w];
         const ScenarioDev &s = scen[item.x];
         ScenarioCtl *ctl = s.ctl;
@@ -263,30 +720,42 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         const bool x_ghost_lo = !s.periodic && gx == 0, x_ghost_hi = !s.periodic && gx == nx;
         const bool x_nolim = (gx < 2) || (gx > nx - 2);
         const bool sponge = (s.sp_left | s.sp_right | s.sp_up | s.sp_low) != 0;
-        float local_min = FLT_MAX;
+        float local_min = FLT_MAX;    // phase 1: upper half tile's depth minimum; else dt
+        float local_min1 = FLT_MAX;   // phase 1: lower half tile's depth minimum
         bool bad = false;
 
         if (x0 < nx) {
+            constexpr bool DIAG = (PHASE == 1);
             Cell c0 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 2, ny) * pitch + col);
             Cell c1 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 1, ny) * pitch + col);
-            Cell c2 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0, ny) * pitch + col);
-            Cell c3 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 + 1, ny) * pitch + col);
-            Cell c4 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 + 2, ny) * pitch + col);
-            RawCell n1 = load_raw(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 + 3, ny) * pitch + col);
+            Cell c2, c3, c4;
+            {
+                // rows y0 .. y0+2 with their diagnostics (rows below the grid are clamped and skipped)
+                const RawCell r0 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0, ny) * pitch + col, has_cell);
+                const RawCell r1 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 1, ny) * pitch + col,
+                                                  has_cell && y0 + 1 < y_end);
+                const RawCell r2 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 2, ny) * pitch + col,
+                                                  has_cell && y0 + 2 < y_end);
+                if (DIAG && has_cell) {
+                    diagnostics(s, r0, (size_t)y0 * pitch + col, t_sec);
+                    if (y0 + 1 < y_end) diagnostics(s, r1, (size_t)(y0 + 1) * pitch + col, t_sec);
+                    if (y0 + 2 < y_end) diagnostics(s, r2, (size_t)(y0 + 2) * pitch + col, t_sec);
+                }
+                c2 = finish(r0);
+                c3 = finish(r1);
+                c4 = finish(r2);
+            }
+            RawCell n1 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 3, ny) * pitch + col,
+                                        has_cell && y0 + 3 < y_end);
             // y edge at the top of the first row (stencil rows y0-2 .. y0+1)
             Contrib top, dummy;
             y_edge<PHASE>(s, c0, c1, c2, c3, y0, dt, dummy, top);
 
             for (int yo = y0; yo < y_end; yo++) {
                 // rows yo+3 (loaded an iteration ago) and yo+4 (now) are in flight
-                const RawCell n2 = load_raw(eta_in, s.dep, qx_in, qy_in, clamp_row(yo + 4, ny) * pitch + col);
+                const RawCell n2 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(yo + 4, ny) * pitch + col,
+                                                  has_cell && yo + 4 < y_end);
                 const size_t idx = (size_t)yo * pitch + col;
-                float em = 0.f, ar = 0.f, ei = 0.f;
-                if (PHASE == 1 && has_cell) {
-                    em = s.eta_max[idx];
-                    ar = s.arr[idx];
-                    ei = s.eta_ini[idx];
-                }
                 // ---- y edge below this row (between yo and yo+1) ----
                 Contrib below, next_top;
                 y_edge<PHASE>(s, c1, c2, c3, c4, yo + 1, dt, below, next_top);
@@ -360,14 +829,11 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                         const float step = (lam < kEps) ? 1e30f : __fdividef(2.f * s.cfl * area, lam);
                         local_min = fminf(local_min, step);
                     } else if (PHASE == 1) {
-                        // diagnostics of the state the step starts from
-                        const float e_old = c2.e, h_old = c2.h;
-                        if (e_old > em && h_old > s.eps_h) s.eta_max[idx] = e_old;
-                        if (ar < 0.f && fabsf(e_old - ei) > s.dif_at) s.arr[idx] = t_sec;
-                        // mass update (src/GPU/Volumen_kernel.cu:111-157)
+                        // mass update (src/GPU/Volumen_kernel.cu:111-157); the
+                        // diagnostics run when a row's loads complete
                         const float acc = ((xr.a + xrr.a) + top.a) + below.a;
                         const float D = c2.D;
-                        float eta = e_old + __fdividef(dt, area) * acc;
+                        float eta = c2.e + __fdividef(dt, area) * acc;
                         if (!(eta + D > 0.f)) eta = -D;
                         if (sponge && ((gx < s.sp_left) || (gx >= nx - s.sp_right) || (yo < s.sp_up) ||
                                        (yo >= ny - s.sp_low))) {
@@ -391,6 +857,8 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                         }
                         if (!isfinite(eta)) bad = true;
                         s.eta[p ^ 1][idx] = eta;
+                        if (yo < y0 + kHalfRows) local_min = fminf(local_min, eta + D);
+                        else local_min1 = fminf(local_min1, eta + D);
                     } else {
                         // momentum update (src/GPU/Volumen_kernel.cu:175-219)
                         const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
@@ -454,30 +922,40 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                 c1 = c2;
                 c2 = c3;
                 c3 = c4;
+                if (DIAG && has_cell && yo + 3 < y_end) diagnostics(s, n1, idx + 3 * pitch, t_sec);
                 c4 = finish(n1);
                 n1 = n2;
             }
         }
         if (bad) atomicOr(&ctl->errors, 1u);
-        if (PHASE == 1) continue;
 
-        // ---- tile min of the local dt -> scenario min; last tile runs the controller ----
-        for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
-        if (lane == 0) red[warp] = local_min;
+        // ---- tile min: phase 1 depth -> tile_hmin (per half); phase 0/2 dt -> scenario min ----
+        for (int o = 16; o > 0; o >>= 1) {
+            local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+            if (PHASE == 1) local_min1 = fminf(local_min1, __shfl_xor_sync(0xffffffffu, local_min1, o));
+        }
+        if (lane == 0) {
+            red[warp] = local_min;
+            if (PHASE == 1) red[WARPS + warp] = local_min1;
+        }
         __syncthreads();
         if (threadIdx.x == 0) {
             float m = red[0];
             for (int k = 1; k < WARPS; k++) m = fminf(m, red[k]);
-            atomicMin(&ctl->dt_bits, __float_as_uint(m));
-            __threadfence();
-            const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
-            is_last = (prev == (unsigned)(s.ntiles - 1));
-            if (is_last) {
+            if (PHASE == 1) {
+                float m1 = red[WARPS];
+                for (int k = 1; k < WARPS; k++) m1 = fminf(m1, red[WARPS + k]);
+                s.tile_hmin[p ^ 1][2 * item.y] = m;
+                s.tile_hmin[p ^ 1][2 * item.y + 1] = m1;
+            } else {
+                atomicMin(&ctl->dt_bits, __float_as_uint(m));
+            }
+            if (PHASE == 0) {
+                // initial dt: the last tile stores the min and resets the counters
                 __threadfence();
-                if (PHASE == 2) {
-                    controller(s);
-                } else {
-                    // initial dt: store the min and reset the counters
+                const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
+                if (prev == (unsigned)(s.ntiles - 1)) {
+                    __threadfence();
                     ctl->dt = (double)__uint_as_float(atomicOr(&ctl->dt_bits, 0u));
                     ctl->dt_bits = 0x7f7fffffu;
                     ctl->tiles_done = 0u;
@@ -488,23 +966,70 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
     }
 }
 
-size_t step_smem_bytes() { return sizeof(float) * WARPS + sizeof(int); }
-
-void launch_step_phase(int phase, const ScenarioDev *scen, const int2 *work, const int *nwork, int grid, cudaStream_t st)
+// Step controller of every running scenario, after both phase-2 kernels.
+__global__ void controller_kernel(const ScenarioDev *__restrict__ scen, int nslots)
 {
-    switch (phase) {
-    case 0: step_kernel<0><<<grid, NT, 0, st>>>(scen, work, nwork); break;
-    case 1: step_kernel<1><<<grid, NT, 0, st>>>(scen, work, nwork); break;
-    default: step_kernel<2><<<grid, NT, 0, st>>>(scen, work, nwork); break;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nslots) return;
+    const ScenarioDev &s = scen[i];
+    if (!s.ctl || s.ctl->status != kRunning) return;
+    controller(s);
+}
+
+
+void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
+{
+    switch (k) {
+    case 0:
+        deep_kernel<1><<<L.deep_grid[0], DNT, deep_smem_bytes(1), st>>>(L.scen, L.work, L.lists);
+        break;
+    case 1: step_kernel<1><<<L.grid, NT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    case 2:
+        cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
+        classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0);
+        break;
+    case 3:
+        deep_kernel<2><<<L.deep_grid[1], DNT, deep_smem_bytes(2), st>>>(L.scen, L.work, L.lists);
+        break;
+    case 4: step_kernel<2><<<L.grid, NT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    default: controller_kernel<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.scen, L.nslots); break;
     }
 }
 
-cudaError_t configure_step_kernels() { return cudaSuccess; }
+void launch_initial_dt(const StepLaunch &L, cudaStream_t st)
+{
+    step_kernel<0><<<L.grid, NT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap);
+}
+
+void launch_lists_all_general(const StepLaunch &L, cudaStream_t st)
+{
+    cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
+    classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 1);
+}
+
+cudaError_t configure_step_kernels()
+{
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(deep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deep_smem_bytes(1))))
+        return e;
+    if ((e = cudaFuncSetAttribute(deep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deep_smem_bytes(2))))
+        return e;
+    if ((e = cudaFuncSetAttribute(deep_kernel<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
+    return cudaFuncSetAttribute(deep_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
 
 int step_blocks_per_sm()
 {
     int n = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2>, NT, 0);
+    return n;
+}
+
+int deep_blocks_per_sm(int phase)
+{
+    int n = 0;
+    if (phase == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<1>, DNT, deep_smem_bytes(1));
+    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<2>, DNT, deep_smem_bytes(2));
     return n;
 }
 

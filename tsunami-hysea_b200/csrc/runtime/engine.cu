@@ -4,13 +4,15 @@
 // thy_session_* / thy_device_*.
 //
 // The time loop stays on the device: dt, the simulated time and the event
-// checks live in a per-scenario control block updated by the last tile of
-// each phase-2 launch, so steps are launched in graph chunks with one host
+// checks live in a per-scenario control block updated by the controller
+// launch that ends each step, so steps are launched in graph chunks with one host
 // synchronisation per chunk instead of one blocking copy per step.  When an
 // event is due (fault time, snapshot time, gauge time) the controller pauses
 // the scenario; later launches of the chunk do nothing for it, and the host
 // performs the event exactly at that step before resuming.
 #include "engine.h"
+
+#include <cuda.h>
 
 #include <algorithm>
 #include <chrono>
@@ -61,6 +63,8 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
     size_t b = 10 * pitch * ny * sizeof(float);          // fields
     b += (size_t)(5 * ny + 1) * sizeof(float);           // row tables
     b += 3 * (size_t)nx * ny * sizeof(float);            // output staging
+    b += 4 * (size_t)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * sizeof(float);   // tile minima
+    b += kNumMaps * sizeof(TmaMap) + (size_t)(ny + 1) * sizeof(float4);
     if (has_faults) b += (size_t)nx * ny * sizeof(double);
     return b + 4096;
 }
@@ -79,6 +83,9 @@ DevScenario::~DevScenario()
     cudaFree(d_gauge);
     cudaFree(d_out);
     cudaFree(fault_times_d);
+    cudaFree(hmin);
+    cudaFree(tmaps);
+    cudaFree(rowpack);
 }
 
 int DevScenario::setup(const thy_problem *p, cudaStream_t st)
@@ -89,6 +96,7 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     ny = p->ny;
     pitch = round_up(nx, 32);
     plane = (size_t)pitch * ny;
+    if (plane >= (size_t)1 << 31) return THY_ERR_INVALID;   // cell offsets are 32-bit in the kernels
     const size_t n = (size_t)nx * ny;
     Hs = p->H;
     Qs = p->Q;
@@ -146,8 +154,16 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
             dla[y] = (float)p->dlat[y];
         }
         for (int y = 0; y <= ny; y++) dlo[y] = (float)p->dlon[y];
+        std::vector<float4> pk((size_t)ny + 1);
+        for (int y = 0; y <= ny; y++) {
+            const bool cell = y < ny;
+            pk[y] = make_float4(cell ? cosr[y] : 1.f, cell ? ilc[y] : 0.f, cell ? ar[y] : 1.f, dlo[y]);
+        }
+        THY_CK(cudaMalloc(&rowpack, pk.size() * sizeof(float4)));
         THY_CK(cudaMemcpyAsync(rows, r.data(), r.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        THY_CK(cudaMemcpyAsync(rowpack, pk.data(), pk.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
         THY_CK(cudaStreamSynchronize(st));
+        desc.rowpack = rowpack;
         desc.row.cosphi = rows;
         desc.row.ilcos = rows + ny;
         desc.row.area = rows + 2 * ny;
@@ -161,6 +177,9 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.tiles_x = (nx + kTileX - 1) / kTileX;
     desc.tiles_y = (ny + kTileY - 1) / kTileY;
     desc.ntiles = desc.tiles_x * desc.tiles_y;
+    THY_CK(cudaMalloc(&hmin, 4 * (size_t)desc.ntiles * sizeof(float)));
+    desc.tile_hmin[0] = hmin;
+    desc.tile_hmin[1] = hmin + 2 * desc.ntiles;
     desc.periodic = (std::fabs(p->border_left - 2.0) < 2.220446049250313e-16) &&
                     (std::fabs(p->border_right - 2.0) < 2.220446049250313e-16);
     desc.b_up = (float)p->border_up;
@@ -189,6 +208,7 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.eta_max = fields + 7 * plane;
     desc.arr = fields + 8 * plane;
     desc.eta_ini = fields + 9 * plane;
+    if (const int rc = encode_tensor_maps(st)) return rc;
 
     // dimensionless double state -> FP32 device state
     {
@@ -203,6 +223,7 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
         }
         launch_init_state(&desc, nullptr, tmp, tmp + n, hasq ? tmp + 2 * n : nullptr, hasq ? tmp + 3 * n : nullptr, Hmin, st);
         THY_CK(cudaGetLastError());
+        THY_CK(invalidate_tile_minima(st));
         THY_CK(cudaStreamSynchronize(st));
         cudaFree(tmp);
     }
@@ -230,6 +251,75 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     return THY_OK;
 }
 
+// 2D tensor maps of the field planes for the deep-water kernels' TMA
+// staging: state planes boxed kStageW x kStageRows, diagnostics kTileX x
+// kHalfRows, zero fill outside the grid.  A grid with fewer than three tiles
+// in either direction has no deep tile and gets no maps.
+// The driver's encoder is looked up through the runtime, so the library has
+// no link-time dependency on libcuda.
+using EncodeTiledFn = CUresult (*)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_tiled_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
+
+int DevScenario::encode_tensor_maps(cudaStream_t st)
+{
+    desc.tmap = nullptr;
+    if (desc.tiles_x < 3 || desc.tiles_y < 3) return THY_OK;
+    static_assert(sizeof(TmaMap) == sizeof(CUtensorMap), "opaque map size");
+    const EncodeTiledFn encode = encode_tiled_fn();
+    if (!encode) {
+        set_last_cuda_error(cudaErrorSymbolNotFound, "cuTensorMapEncodeTiled entry point", __FILE__, __LINE__);
+        return THY_ERR_CUDA;
+    }
+    CUtensorMap h[kNumMaps];
+    float *base[kNumMaps] = {desc.eta[0], desc.eta[1], desc.qx[0], desc.qx[1], desc.qy[0], desc.qy[1],
+                             desc.dep, desc.eta_max, desc.arr, desc.eta_ini};
+    for (int k = 0; k < kNumMaps; k++) {
+        const bool diag = k >= kMapEtaMax;
+        const cuuint64_t dims[2] = {(cuuint64_t)nx, (cuuint64_t)ny};
+        const cuuint64_t strides[1] = {(cuuint64_t)pitch * sizeof(float)};
+        const cuuint32_t box[2] = {(cuuint32_t)(diag ? kTileX : kStageW), (cuuint32_t)(diag ? kHalfRows : kStageRows)};
+        const cuuint32_t estr[2] = {1, 1};
+        const CUresult r = encode(&h[k], CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, base[k], dims, strides, box,
+                                                  estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                                                  CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+        if (r != CUDA_SUCCESS) {
+            char what[64];
+            snprintf(what, sizeof(what), "cuTensorMapEncodeTiled returned %d", (int)r);
+            set_last_cuda_error(cudaErrorInvalidValue, what, __FILE__, __LINE__);
+            return THY_ERR_CUDA;
+        }
+    }
+    THY_CK(cudaMalloc(&tmaps, kNumMaps * sizeof(TmaMap)));
+    THY_CK(cudaMemcpyAsync(tmaps, h, kNumMaps * sizeof(TmaMap), cudaMemcpyHostToDevice, st));
+    THY_CK(cudaStreamSynchronize(st));
+    desc.tmap = tmaps;
+    return THY_OK;
+}
+
+// The state changed outside phase 1: no tile counts as deep until phase 1
+// has measured the tile minima again (all-ones bytes are NaN floats).
+cudaError_t DevScenario::invalidate_tile_minima(cudaStream_t st)
+{
+    return cudaMemsetAsync(hmin, 0xff, 4 * (size_t)desc.ntiles * sizeof(float), st);
+}
+
 int DevScenario::upload_ctl(cudaStream_t st)
 {
     THY_CK(cudaMemcpyAsync(ctl, &hctl, sizeof(ScenarioCtl), cudaMemcpyHostToDevice, st));
@@ -255,6 +345,7 @@ int DevScenario::apply_due_faults(cudaStream_t st)
         THY_CK(cudaMemcpyAsync(ctl, &hctl, sizeof(ScenarioCtl), cudaMemcpyHostToDevice, st));
         launch_apply_deformation(&desc, def, crop_flag, crop_value, maxbits, st);
         THY_CK(cudaGetLastError());
+        THY_CK(invalidate_tile_minima(st));
         hctl.fault_next++;
     }
     return THY_OK;
@@ -347,10 +438,14 @@ Batch::~Batch()
     cudaFree(d_table);
     cudaFree(d_work);
     cudaFree(d_nwork);
+    cudaFree(d_lists);
     cudaFree(d_ctl);
     cudaFreeHost(h_ctl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
+    if (st_side) cudaStreamDestroy(st_side);
 }
 
 int Batch::init(int cap, int max_work, cudaStream_t stream)
@@ -363,8 +458,13 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     THY_CK(cudaMallocHost(&h_ctl, cap * sizeof(ScenarioCtl)));
     THY_CK(cudaMalloc(&d_work, std::max(max_work, 1) * sizeof(int2)));
     THY_CK(cudaMalloc(&d_nwork, sizeof(int)));
+    THY_CK(cudaMalloc(&d_lists, (2 + 2 * (size_t)std::max(max_work, 1)) * sizeof(int)));
+    THY_CK(cudaMemsetAsync(d_lists, 0, 2 * sizeof(int), st));
     THY_CK(cudaEventCreate(&ev0));
     THY_CK(cudaEventCreate(&ev1));
+    THY_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+    THY_CK(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+    THY_CK(cudaStreamCreateWithFlags(&st_side, cudaStreamNonBlocking));
     std::vector<ScenarioCtl> z(cap);
     for (auto &c : z) { std::memset(&c, 0, sizeof(c)); c.status = kIdle; }
     THY_CK(cudaMemcpyAsync(d_ctl, z.data(), cap * sizeof(ScenarioCtl), cudaMemcpyHostToDevice, st));
@@ -411,8 +511,11 @@ int Batch::rebuild()
     }
     if ((int)work.size() > work_capacity) {
         cudaFree(d_work);
+        cudaFree(d_lists);
+        d_lists = nullptr;
         work_capacity = (int)work.size();
         THY_CK(cudaMalloc(&d_work, work_capacity * sizeof(int2)));
+        THY_CK(cudaMalloc(&d_lists, (2 + 2 * (size_t)work_capacity) * sizeof(int)));
     }
     nwork = (int)work.size();
     THY_CK(cudaMemcpyAsync(d_table, table.data(), capacity * sizeof(ScenarioDev), cudaMemcpyHostToDevice, st));
@@ -421,20 +524,59 @@ int Batch::rebuild()
     THY_CK(cudaStreamSynchronize(st));
     const int bps = std::max(1, step_blocks_per_sm());
     grid = std::max(1, std::min(nwork, device_sm_count() * bps * 8));
+    for (int ph = 0; ph < 2; ph++)
+        deep_grid[ph] = std::max(1, std::min(2 * nwork, device_sm_count() * std::max(1, deep_blocks_per_sm(ph + 1))));
+    if (int rc = reset_lists()) return rc;
     if (gexec) {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
     }
+    // Each phase's general and deep-water kernels step disjoint tiles and
+    // share only atomically updated scenario fields, so they are two
+    // branches of the graph: the deep tiles fill the SMs the general
+    // kernel's last wave leaves idle.
+    const StepLaunch L = params();
     cudaGraph_t g;
     THY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     for (int k = 0; k < chunk; k++) {
-        launch_step_phase(1, d_table, d_work, d_nwork, grid, st);
-        launch_step_phase(2, d_table, d_work, d_nwork, grid, st);
+        for (int ph = 0; ph < 2; ph++) {
+            THY_CK(cudaEventRecord(ev_fork, st));
+            THY_CK(cudaStreamWaitEvent(st_side, ev_fork, 0));
+            launch_step_kernel(3 * ph + 1, L, st);        // general
+            launch_step_kernel(3 * ph, L, st_side);       // deep
+            THY_CK(cudaEventRecord(ev_join, st_side));
+            THY_CK(cudaStreamWaitEvent(st, ev_join, 0));
+            if (ph == 0) launch_step_kernel(2, L, st);   // classification for phase 2 and the next phase 1
+        }
+        launch_step_kernel(5, L, st);                     // controller
     }
     THY_CK(cudaStreamEndCapture(st, &g));
     cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
     cudaGraphDestroy(g);
     THY_CK(e);
+    return THY_OK;
+}
+
+StepLaunch Batch::params() const
+{
+    StepLaunch L;
+    L.scen = d_table;
+    L.work = d_work;
+    L.nwork = d_nwork;
+    L.lists = d_lists;
+    L.cap = work_capacity;
+    L.grid = grid;
+    L.deep_grid[0] = deep_grid[0];
+    L.deep_grid[1] = deep_grid[1];
+    L.classify_grid = std::max(1, std::min((nwork + 255) / 256, 4 * device_sm_count()));
+    L.nslots = capacity;
+    return L;
+}
+
+int Batch::reset_lists()
+{
+    launch_lists_all_general(params(), st);
+    THY_CK(cudaGetLastError());
     return THY_OK;
 }
 
@@ -450,7 +592,7 @@ int Batch::run_chunk(bool timed)
         THY_CK(cudaEventElapsedTime(&ms, ev0, ev1));
         device_ms += ms;
     }
-    launches += 2LL * chunk;
+    launches += (long long)kLaunchesPerStep * chunk;
     for (int i = 0; i < capacity; i++)
         if (members[i]) members[i]->hctl = h_ctl[i];
     return THY_OK;
@@ -463,7 +605,7 @@ static int initial_dt(Batch &b)
     int rc;
     for (auto *s : b.members)
         if (s && (rc = s->upload_ctl(b.st))) return rc;
-    launch_step_phase(0, b.d_table, b.d_work, b.d_nwork, b.grid, b.st);
+    launch_initial_dt(b.params(), b.st);
     THY_CK(cudaGetLastError());
     THY_CK(cudaMemcpyAsync(b.h_ctl, b.d_ctl, b.capacity * sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, b.st));
     THY_CK(cudaStreamSynchronize(b.st));
@@ -575,6 +717,7 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
             if (s.max_steps >= 0 && s.hctl.step >= s.max_steps) break;
             if (s.hctl.status == kFailed) { rc = THY_ERR_NONFINITE; goto out; }
             if ((rc = handle_events(s, o, st))) goto out;
+            if ((rc = b.reset_lists())) goto out;
             s.hctl.status = kRunning;
             s.hctl.events = 0;
             if ((rc = s.upload_ctl(st))) goto out;
@@ -594,6 +737,8 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
                 stats->kernel_launches = b.launches;
                 stats->snapshots = s.snapshots;
                 stats->series_samples = s.series;
+                stats->tiles = s.hctl.step * (long long)s.desc.ntiles;
+                stats->deep_tiles = (long long)s.hctl.tiles_deep;
             }
         }
         rc = s.finish(o, st);
@@ -626,7 +771,7 @@ extern "C" int thy_session_open(const thy_problem *p, thy_session **out)
     q.max_steps = 0;
     if ((rc = S->b.init(1, (p->nx / kTileX + 2) * (p->ny / kTileY + 2), S->st)) || (rc = S->b.attach(&S->s)) ||
         (rc = S->s.setup(&q, S->st)) || (rc = S->b.rebuild()) || (rc = initial_dt(S->b)) ||
-        (rc = S->s.apply_due_faults(S->st))) {
+        (rc = S->s.apply_due_faults(S->st)) || (rc = S->b.reset_lists())) {
         cudaStream_t st = S->st;
         delete S;
         cudaStreamDestroy(st);
@@ -658,47 +803,68 @@ extern "C" int thy_session_steps(thy_session *S, long long steps, double *device
 }
 
 // Per-kernel device time: `steps` steps launched one kernel at a time with
-// CUDA events around each launch on the session's stream.  Returns the
-// average duration (ms) of the phase-1 and phase-2 launches.
-extern "C" int thy_session_profile(thy_session *S, long long steps, double *phase1_ms, double *phase2_ms)
+// CUDA events around each launch on the session's stream.  ms_per_launch
+// receives the average duration (ms) of each of the kLaunchesPerStep launches
+// of a step (deep phase 1, general phase 1, classification, deep phase 2,
+// general phase 2, controller).
+extern "C" int thy_session_profile_launches(thy_session *S, long long steps, double *ms_per_launch)
 {
     if (!S || steps <= 0) return THY_ERR_INVALID;
     DevScenario &s = S->s;
     Batch &b = S->b;
+    constexpr int NL = kLaunchesPerStep;
+    const StepLaunch L = b.params();
     int rc;
     s.hctl.max_steps = s.hctl.step + steps;
     s.hctl.status = kRunning;
     s.hctl.events = 0;
     if ((rc = s.upload_ctl(S->st))) return rc;
-    std::vector<cudaEvent_t> ev(3 * steps);
+    std::vector<cudaEvent_t> ev((NL + 1) * steps);
     for (auto &e : ev) THY_CK(cudaEventCreate(&e));
     for (long long k = 0; k < steps; k++) {
-        THY_CK(cudaEventRecord(ev[3 * k], S->st));
-        launch_step_phase(1, b.d_table, b.d_work, b.d_nwork, b.grid, S->st);
-        THY_CK(cudaEventRecord(ev[3 * k + 1], S->st));
-        launch_step_phase(2, b.d_table, b.d_work, b.d_nwork, b.grid, S->st);
-        THY_CK(cudaEventRecord(ev[3 * k + 2], S->st));
+        for (int j = 0; j < NL; j++) {
+            THY_CK(cudaEventRecord(ev[(NL + 1) * k + j], S->st));
+            launch_step_kernel(j, L, S->st);
+        }
+        THY_CK(cudaEventRecord(ev[(NL + 1) * k + NL], S->st));
     }
     THY_CK(cudaGetLastError());
     THY_CK(cudaStreamSynchronize(S->st));
-    double t1 = 0, t2 = 0;
-    for (long long k = 0; k < steps; k++) {
-        float a = 0, c = 0;
-        THY_CK(cudaEventElapsedTime(&a, ev[3 * k], ev[3 * k + 1]));
-        THY_CK(cudaEventElapsedTime(&c, ev[3 * k + 1], ev[3 * k + 2]));
-        t1 += a;
-        t2 += c;
-    }
+    double t[NL] = {};
+    for (long long k = 0; k < steps; k++)
+        for (int j = 0; j < NL; j++) {
+            float a = 0;
+            THY_CK(cudaEventElapsedTime(&a, ev[(NL + 1) * k + j], ev[(NL + 1) * k + j + 1]));
+            t[j] += a;
+        }
     for (auto &e : ev) cudaEventDestroy(e);
-    b.launches += 2 * steps;
+    b.launches += (long long)NL * steps;
     if ((rc = s.download_ctl(S->st))) return rc;
     THY_CK(cudaStreamSynchronize(S->st));
-    if (phase1_ms) *phase1_ms = t1 / steps;
-    if (phase2_ms) *phase2_ms = t2 / steps;
+    if (ms_per_launch)
+        for (int j = 0; j < NL; j++) ms_per_launch[j] = t[j] / steps;
     return s.hctl.status == kFailed ? THY_ERR_NONFINITE : THY_OK;
 }
 
+// Average device time of phase 1 and phase 2 (each the sum of its launches).
+extern "C" int thy_session_profile(thy_session *S, long long steps, double *phase1_ms, double *phase2_ms)
+{
+    double t[kLaunchesPerStep] = {};
+    const int rc = thy_session_profile_launches(S, steps, t);
+    if (phase1_ms) *phase1_ms = t[0] + t[1] + t[2];
+    if (phase2_ms) *phase2_ms = t[3] + t[4] + t[5];
+    return rc;
+}
+
 extern "C" long long thy_session_launches(const thy_session *S) { return S ? S->b.launches : 0; }
+
+extern "C" int thy_session_tiles(const thy_session *S, long long *tiles, long long *deep_tiles)
+{
+    if (!S) return THY_ERR_INVALID;
+    if (tiles) *tiles = S->s.hctl.step * (long long)S->s.desc.ntiles;
+    if (deep_tiles) *deep_tiles = (long long)S->s.hctl.tiles_deep;
+    return THY_OK;
+}
 
 extern "C" int thy_session_fetch(thy_session *S, float *max_height, float *eta, float *ux, float *uy)
 {

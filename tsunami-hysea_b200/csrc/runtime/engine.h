@@ -44,6 +44,9 @@ struct DevScenario {
     float *d_gauge = nullptr;      // 4 floats per gauge
     float *d_out = nullptr;        // 3 planes nx*ny for snapshots / outputs
     double *fault_times_d = nullptr;
+    float *hmin = nullptr;         // 2 parities x 2 ntiles half-tile depth minima (desc.tile_hmin)
+    TmaMap *tmaps = nullptr;       // kNumMaps tensor maps of the field planes (desc.tmap)
+    float4 *rowpack = nullptr;     // ny+1 packed row metrics (desc.rowpack)
     ScenarioCtl *ctl = nullptr;    // device control block (owned by the batch slot)
     ScenarioDev desc{};            // descriptor (device pointers), host copy
     // problem data kept on the host
@@ -68,6 +71,8 @@ struct DevScenario {
     int upload_ctl(cudaStream_t st);
     int download_ctl(cudaStream_t st);                   // async into hctl (pinned by the batch)
     int apply_due_faults(cudaStream_t st);               // faults with time <= t (the loop's first action)
+    cudaError_t invalidate_tile_minima(cudaStream_t st);
+    int encode_tensor_maps(cudaStream_t st);
     int extract(int field, float *host_out, cudaStream_t st);
     int snapshot(const thy_outputs *o, cudaStream_t st);
     int sample_gauges(const thy_outputs *o, cudaStream_t st);
@@ -75,20 +80,24 @@ struct DevScenario {
 };
 
 // A set of scenarios stepped together: one work list over all their tiles,
-// one CUDA graph of `chunk` steps (2 launches per step).
+// one CUDA graph of `chunk` steps (kLaunchesPerStep launches per step).
 struct Batch {
     std::vector<DevScenario *> members;
     ScenarioDev *d_table = nullptr;
     int2 *d_work = nullptr;
     int *d_nwork = nullptr;
+    int *d_lists = nullptr;            // deep / general lists of the current step (StepLaunch::lists)
     ScenarioCtl *d_ctl = nullptr;      // slots
     ScenarioCtl *h_ctl = nullptr;      // pinned mirror
     int capacity = 0;
     int work_capacity = 0;
     int nwork = 0;
     int grid = 0;
+    int deep_grid[2] = {1, 1};
     int chunk = 16;
     cudaStream_t st = nullptr;
+    cudaStream_t st_side = nullptr;    // second branch of the captured graph (deep-water kernels)
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     cudaGraphExec_t gexec = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double device_ms = 0;
@@ -100,6 +109,8 @@ struct Batch {
     int detach(DevScenario *s);
     int rebuild();                    // tables + work list of RUNNING members; recapture the graph
     int run_chunk(bool timed);       // one graph launch + control download (synchronous)
+    StepLaunch params() const;
+    int reset_lists();               // all items general: after the host changed a member's state
 };
 
 int ensure_device();

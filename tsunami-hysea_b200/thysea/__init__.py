@@ -144,7 +144,7 @@ def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = Tru
                          bathy=pts["series_bathy"][:pc.npoints])
     res.update(iterations=st.steps, final_time=st.final_time_s, first_dt=st.first_dt_s,
                loop_seconds=st.loop_seconds, device_ms=st.device_loop_ms, kernel_launches=st.kernel_launches,
-               nsnaps=st.snapshots, nseries=st.series_samples)
+               nsnaps=st.snapshots, nseries=st.series_samples, tiles=st.tiles, deep_tiles=st.deep_tiles)
     return res
 
 
@@ -176,8 +176,22 @@ class Session:
         _check(_ffi.lib().thy_session_profile(self._h, k, ctypes.byref(a), ctypes.byref(b)), "thy_session_profile")
         return a.value, b.value
 
+    def profile_launches(self, k: int):
+        """k individually launched steps; average ms of each launch of a step
+        (deep phase 1, general phase 1, classification, deep phase 2, general
+        phase 2, controller)."""
+        t = (ctypes.c_double * 6)()
+        _check(_ffi.lib().thy_session_profile_launches(self._h, k, t), "thy_session_profile_launches")
+        return list(t)
+
     def launches(self) -> int:
         return int(_ffi.lib().thy_session_launches(self._h))
+
+    def tiles(self):
+        """(phase-2 tiles stepped, of which by the deep-water kernels)"""
+        t, d = ctypes.c_longlong(), ctypes.c_longlong()
+        _check(_ffi.lib().thy_session_tiles(self._h, ctypes.byref(t), ctypes.byref(d)), "thy_session_tiles")
+        return t.value, d.value
 
     def fetch(self):
         c = self.prep.c
