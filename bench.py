@@ -40,7 +40,7 @@ sys.path.insert(0, os.path.join(ROOT, "tsunami-hysea_b200"))
 METRIC = "cell-updates/s"
 BYTES_PHASE1 = 36   # eta, dep, qx, qy read (16) + eta written (4) + max-height/arrival/initial eta read, max written (16)
 BYTES_PHASE2 = 24   # eta, dep, qx, qy read (16) + qx, qy written (8)
-TILE_CELLS = 112 * 32   # cells of a full tile (kTileX x kTileY)
+UNIT_CELLS = 112 * 16   # cells of a work unit (half tile, kTileX x kHalfRows)
 
 
 def env_int(k, d):
@@ -233,17 +233,19 @@ def run_ours(a, dist: Dist):
     total_cells = dist.sum(float(cells * a.steps))
     value = total_cells / dev_s
     # per-kernel device time for the roofline (individually launched steps);
-    # each kernel's algorithmic bytes count the cells it steps: deep tiles are
-    # interior tiles of TILE_CELLS cells, the general kernels step the rest
-    t0_tiles, t0_deep = sess.tiles()
+    # each kernel's algorithmic bytes count the cells it steps: deep units are
+    # interior units of UNIT_CELLS cells, dry land units are skipped, the
+    # general kernels step the rest
+    t0_units, t0_deep, t0_dry = sess.tiles()
     prof_steps = 32
     ms6 = sess.profile_launches(prof_steps)
-    t1_tiles, t1_deep = sess.tiles()
+    t1_units, t1_deep, t1_dry = sess.tiles()
     sess.close()
-    deep_frac = (t1_deep - t0_deep) / max(1, t1_tiles - t0_tiles)
-    ntiles = (t1_tiles - t0_tiles) // prof_steps
-    cells_deep = (t1_deep - t0_deep) / prof_steps * TILE_CELLS
-    cells_gen = cells - cells_deep
+    nunits = max(1, t1_units - t0_units)
+    deep_frac = (t1_deep - t0_deep) / nunits
+    dry_frac = (t1_dry - t0_dry) / nunits
+    cells_deep = (t1_deep - t0_deep) / prof_steps * UNIT_CELLS
+    cells_gen = max(0.0, cells - cells_deep - (t1_dry - t0_dry) / prof_steps * UNIT_CELLS)
     peak, peak_kind = measured_peak()
     kern = {"deep_phase1": (ms6[0], BYTES_PHASE1, cells_deep), "general_phase1": (ms6[1], BYTES_PHASE1, cells_gen),
             "deep_phase2": (ms6[3], BYTES_PHASE2, cells_deep), "general_phase2": (ms6[4], BYTES_PHASE2, cells_gen)}
@@ -257,7 +259,8 @@ def run_ours(a, dist: Dist):
                 "algorithmic_bytes_per_cell": bpc, "cells_per_launch": int(kcells),
                 "per_kernel_ms": {**{k: round(v[0], 5) for k, v in kern.items()}, "classify": round(ms6[2], 5),
                                   "controller": round(ms6[5], 5)},
-                "deep_tile_fraction": round(deep_frac, 4), "tiles": int(ntiles),
+                "deep_unit_fraction": round(deep_frac, 4), "dry_unit_fraction": round(dry_frac, 4),
+                "units": int(nunits // prof_steps),
                 "step_frac_of_peak": round((BYTES_PHASE1 + BYTES_PHASE2) * cells / (step_ms * 1e-3) / 1e9 / peak, 4)}
     # end to end through the public API on host buffers: full 3600 s runs
     e2e = None

@@ -122,8 +122,9 @@ typedef struct thy_stats {
     double device_loop_ms;    /* device time of the stepping kernels (CUDA events) */
     long long kernel_launches;/* kernels launched by the time loop */
     int snapshots, series_samples;
-    long long tiles;          /* phase-2 tiles stepped (steps x tiles of the grid) */
-    long long deep_tiles;     /* ... of which by the deep-water kernels */
+    long long tiles;          /* work units (112 x 16-cell half tiles) x steps */
+    long long deep_tiles;     /* ... stepped by the deep-water kernels (phase 2) */
+    long long dry_tiles;      /* ... skipped as settled dry land */
 } thy_stats;
 
 /* Library / device. */
@@ -198,8 +199,9 @@ int thy_session_profile(thy_session *s, long long steps, double *phase1_ms, doub
    deep/general classification, deep phase 2, general phase 2, step controller */
 int thy_session_profile_launches(thy_session *s, long long steps, double *ms_per_launch);
 long long thy_session_launches(const thy_session *s);   /* stepping kernels launched so far */
-/* phase-2 tiles stepped so far, and how many of them by the deep-water kernels */
-int thy_session_tiles(const thy_session *s, long long *tiles, long long *deep_tiles);
+/* work units (112 x 16-cell half tiles) x steps so far, of which stepped by
+   the deep-water kernels, and skipped as settled dry land */
+int thy_session_tiles(const thy_session *s, long long *tiles, long long *deep_tiles, long long *dry_tiles);
 double thy_session_time(const thy_session *s);    /* simulated time (s) */
 void thy_session_close(thy_session *s);
 

@@ -66,7 +66,8 @@ struct ScenarioCtl {
     unsigned int errors;       // non-finite values seen
     int pad_;
     const double *fault_times; // nfaults fault times (s), sorted, device memory
-    unsigned long long tiles_deep;   // phase-2 tiles stepped by the deep-water kernels
+    unsigned long long units_deep;   // work units stepped by the deep-water kernels (phase 2)
+    unsigned long long units_dry;    // work units skipped as dry land (classifications)
 };
 
 // Opaque 128-byte TMA tensor map (CUtensorMap), 64-byte aligned in device memory.
@@ -98,10 +99,14 @@ struct ScenarioDev {
     float *eta_max;
     float *arr;
     float *eta_ini;
-    // per half tile (rows 0-15 / 16-31 of tile t at 2t / 2t+1): minimum water
-    // depth eta + dep over its cells, written by phase 1 for the state it
-    // produces (index parity^1); NaN = unknown
-    float *tile_hmin[2];
+    // per work unit (half tile of kTileX x kHalfRows cells; unit (tx, uy) at
+    // uy * tiles_x + tx): {min, max} of the water depth eta + dep over its
+    // cells, written by phase 1 for the state it produces (index parity^1);
+    // NaN = unknown
+    float2 *usum[2];
+    // per unit: consecutive classifications that found its 3 x 3 unit
+    // neighbourhood dry (saturating)
+    unsigned char *dry_age;
     // TMA tensor maps of the field planes (kMap* order), null when the grid
     // is too small to have deep tiles
     const struct TmaMap *tmap;

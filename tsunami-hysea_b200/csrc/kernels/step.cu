@@ -260,26 +260,61 @@ __device__ __forceinline__ void y_edge(const ScenarioDev &s, const Cell &m, cons
     }
 }
 
-// Deep-tile predicate; hmin = half-tile minimum depths of the state the phase
-// reads.  The geometric tests imply 1 <= tx <= tiles_x - 2 and
-// 1 <= ty <= tiles_y - 2; the stencil reaches two cells beyond the tile, so
-// the lower half of the tile row above, both halves of the tile's own row and
-// the upper half of the row below are checked, for the tile and its left and
-// right neighbours.  Unknown minima are NaN and fail the comparison.
-__device__ __forceinline__ bool tile_is_deep(const ScenarioDev &s, const float *__restrict__ hmin, int tx, int ty)
+// ---------------------------------------------------------------------------
+// Work units and their classes.  A unit is a half tile (kTileX x kHalfRows
+// cells); work-list entry w (scenario, tile) holds units 2w (upper half) and
+// 2w+1 (lower half).  Phase 1 records each unit's depth {min, max}; from
+// those of the 3 x 3 units around (which cover the two-cell stencil ring),
+//   deep:  every cell of the neighbourhood deeper than hpos, and the unit at
+//          least two cells from the boundaries and outside the sponge
+//          layers - every edge is a pure 2s edge and no cell is dried,
+//          damped or relaxed;
+//   dry:   every cell of the neighbourhood dry (depth 0) at three
+//          consecutive classifications - then both state buffers hold the
+//          scheme's fixed point (eta = -dep, q = 0), which a step would write
+//          again, so the unit is skipped;
+//   general: the rest.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int units_y(const ScenarioDev &s) { return (s.ny + kHalfRows - 1) / kHalfRows; }
+
+// The geometric tests imply 1 <= tx <= tiles_x - 2 and 1 <= uy <= units_y - 2.
+__device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const float2 *__restrict__ sum, int tx, int uy)
 {
     if (!s.tmap) return false;
-    const int x0 = tx * kTileX, y0 = ty * TY;
+    const int x0 = tx * kTileX, yb = uy * kHalfRows;
     if (x0 < max(2, s.sp_left) || x0 + kTileX > s.nx - max(2, s.sp_right)) return false;
-    if (y0 < max(2, s.sp_up) || y0 + TY > s.ny - max(2, s.sp_low)) return false;
-    const float *up = hmin + 2 * ((size_t)(ty - 1) * s.tiles_x + (tx - 1));
-    const float *mid = up + 2 * s.tiles_x, *dn = mid + 2 * s.tiles_x;
+    if (yb < max(2, s.sp_up) || yb + kHalfRows > s.ny - max(2, s.sp_low)) return false;
     const float hp = s.hpos;
     bool ok = true;
-    for (int k = 0; k < 3; k++)
-        ok = ok && (up[2 * k + 1] > hp) && (mid[2 * k] > hp) && (mid[2 * k + 1] > hp) && (dn[2 * k] > hp);
+    for (int dy = -1; dy <= 1; dy++) {
+        const float2 *r = sum + (size_t)(uy + dy) * s.tiles_x + tx;
+        ok = ok && (r[-1].x > hp) && (r[0].x > hp) && (r[1].x > hp);
+    }
     return ok;
 }
+
+// Outside the grid counts as dry (ghost cells copy the boundary cell), except
+// across a periodic x boundary, where the wrapped unit counts.
+__device__ __forceinline__ bool unit_dry(const ScenarioDev &s, const float2 *__restrict__ sum, int tx, int uy)
+{
+    const int ny_u = units_y(s), nx_u = s.tiles_x;
+    bool dry = true;
+    for (int dy = -1; dy <= 1; dy++) {
+        const int y = uy + dy;
+        if (y < 0 || y >= ny_u) continue;
+        for (int dx = -1; dx <= 1; dx++) {
+            int x = tx + dx;
+            if (x < 0 || x >= nx_u) {
+                if (!s.periodic) continue;
+                x = (x + nx_u) % nx_u;
+            }
+            dry = dry && (sum[(size_t)y * nx_u + x].y <= 0.f);
+        }
+    }
+    return dry;
+}
+
+constexpr int kDryAge = 3;   // classifications a unit must stay dry before it is skipped
 
 // ---------------------------------------------------------------------------
 // TMA staging: one elected thread issues 2D tensor copies of a half tile's
@@ -362,7 +397,7 @@ struct DeepRow {
 __host__ __device__ constexpr size_t deep_misc_offset(int phase) { return 2 * deep_stage_bytes(phase); }
 static size_t deep_smem_bytes(int phase)
 {
-    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + DWARPS * sizeof(float);
+    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + 2 * DWARPS * sizeof(float);
 }
 
 // one cell of a staged row (shared memory; the depth is formed here)
@@ -383,33 +418,49 @@ __device__ __forceinline__ Cell staged_cell(const float *st, int i)
 __device__ __forceinline__ const int *deep_items(const int *lists) { return lists + 2; }
 __device__ __forceinline__ const int *general_items(const int *lists, int cap) { return lists + 2 + cap; }
 
-// Splits the work list into deep and general items for the state the next
-// phase reads: after phase 1 of a running scenario that is the state phase 1
-// produced (minima at parity^1), which phase 2 of this step and phase 1 of the
-// next step both read; for a scenario that is not running it is the state at
-// its current parity.  all_general (after any change of the state by the
-// host) puts every item on the general list.  The counts are zeroed before.
+// Splits the work units into deep and general lists (dry units go to
+// neither) for the state the next phase reads: after phase 1 of a running
+// scenario that is the state phase 1 produced (summaries at parity^1), which
+// phase 2 of this step and phase 1 of the next step both read; for a scenario
+// that is not running it is the state at its current parity.  all_general
+// (after the host changed a state) puts every unit on the general list.
+// Units below the grid (the lower half of a last tile row of <= 16 rows) are
+// not listed.  The counts are zeroed before the launch.
 __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                 const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int all_general)
 {
-    const int n = *nwork_ptr;
+    const int n = 2 * *nwork_ptr;
     const int lane = threadIdx.x & 31;
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
-        const int w = base + threadIdx.x;
-        bool deep = false;
-        if (w < n && !all_general) {
-            const int2 item = work[w];
+        const int u = base + threadIdx.x;
+        bool listed = false, deep = false;
+        if (u < n) {
+            const int2 item = work[u >> 1];
             const ScenarioDev &s = scen[item.x];
-            const ScenarioCtl *ctl = s.ctl;
-            const int p = ctl->parity;
-            const int par = (ctl->status == kRunning) ? (p ^ 1) : p;
             const int ty = item.y / s.tiles_x, tx = item.y - ty * s.tiles_x;
-            deep = tile_is_deep(s, s.tile_hmin[par], tx, ty);
+            const int uy = 2 * ty + (u & 1);
+            listed = uy * kHalfRows < s.ny;
+            if (listed && !all_general) {
+                ScenarioCtl *ctl = s.ctl;
+                const bool running = ctl->status == kRunning;
+                const int par = running ? (ctl->parity ^ 1) : ctl->parity;
+                const float2 *sum = s.usum[par];
+                deep = unit_deep(s, sum, tx, uy);
+                const size_t k = (size_t)uy * s.tiles_x + tx;
+                int age = s.dry_age[k];
+                if (running) {
+                    age = (!deep && unit_dry(s, sum, tx, uy)) ? min(age + 1, 255) : 0;
+                    s.dry_age[k] = (unsigned char)age;
+                }
+                if (age >= kDryAge) {
+                    listed = false;
+                    if (running) atomicAdd(&ctl->units_dry, 1ull);
+                }
+            }
         }
         // warp-aggregated appends
-        const unsigned in_range = __ballot_sync(0xffffffffu, w < n);
-        const unsigned dm = __ballot_sync(0xffffffffu, deep && w < n);
-        const unsigned gm = in_range & ~dm;
+        const unsigned dm = __ballot_sync(0xffffffffu, listed && deep);
+        const unsigned gm = __ballot_sync(0xffffffffu, listed && !deep);
         int dbase = 0, gbase = 0;
         if (lane == 0) {
             if (dm) dbase = atomicAdd(&lists[0], __popc(dm));
@@ -418,9 +469,9 @@ __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2
         dbase = __shfl_sync(0xffffffffu, dbase, 0);
         gbase = __shfl_sync(0xffffffffu, gbase, 0);
         const unsigned below = (1u << lane) - 1u;
-        if (w < n) {
-            if (deep) lists[2 + dbase + __popc(dm & below)] = w;
-            else lists[2 + cap + gbase + __popc(gm & below)] = w;
+        if (listed) {
+            if (deep) lists[2 + dbase + __popc(dm & below)] = u;
+            else lists[2 + cap + gbase + __popc(gm & below)] = u;
         }
     }
 }
@@ -446,24 +497,25 @@ __device__ __forceinline__ void y_edge_deep(const ScenarioDev &s, const Cell &a,
     }
 }
 
-// A deep work unit: half `half` of work item `w`.
+// A deep work unit: unit code u = 2 * (work-list index) + half.
 struct DeepUnit {
     const ScenarioDev *s;
-    int tile, half, x0, yb, p;
+    int uidx, x0, yb, p;      // uidx: the unit's index in the scenario's unit grid
     bool run;
 };
 
 __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                              const int *__restrict__ lists, int u)
+                                              const int *__restrict__ lists, int i)
 {
     DeepUnit d;
-    const int2 item = work[deep_items(lists)[u >> 1]];
+    const int u = deep_items(lists)[i];
+    const int2 item = work[u >> 1];
     d.s = &scen[item.x];
-    d.tile = item.y;
-    d.half = u & 1;
     const int ty = item.y / d.s->tiles_x, tx = item.y - ty * d.s->tiles_x;
+    const int uy = 2 * ty + (u & 1);
+    d.uidx = uy * d.s->tiles_x + tx;
     d.x0 = tx * kTileX;
-    d.yb = ty * TY + d.half * kHalfRows;
+    d.yb = uy * kHalfRows;
     const ScenarioCtl *ctl = d.s->ctl;
     d.p = ctl->parity;
     d.run = *((volatile const int *)&ctl->status) == kRunning;
@@ -514,14 +566,14 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
     float *red = reinterpret_cast<float *>(rows + kStageRows);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int strip = warp & 3, group = warp >> 2;
-    const int nunits = 2 * lists[0];
+    const int nunits = lists[0];
     if (blockIdx.x >= nunits) return;
     // TMA destinations must be 128-byte aligned: a misaligned buffer is
     // reported on every scenario of the CTA's units and nothing is copied
     if (smem_addr(dsm) & 127u) {
         if (threadIdx.x == 0)
             for (int u = blockIdx.x; u < nunits; u += gridDim.x)
-                atomicOr(&scen[work[deep_items(lists)[u >> 1]].x].ctl->errors, 4u);
+                atomicOr(&scen[work[deep_items(lists)[u] >> 1].x].ctl->errors, 4u);
         return;
     }
     if (threadIdx.x == 0) {
@@ -574,7 +626,8 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
             const int gx = x0 - 4 + sc;                             // grid column
             const bool has_cell = (lane >= 2) && (lane <= 29);
             const int dcol = strip * 28 - 2 + lane;                 // diagnostics column (cells only)
-            float local_min = FLT_MAX;
+            float local_min = FLT_MAX;    // phase 1: depth minimum; phase 2: dt
+            float local_max = -FLT_MAX;   // phase 1: depth maximum
             bool bad = false;
             int i = r_first * kStageW + sc;
             Cell c = staged_cell(stage, i);
@@ -647,6 +700,7 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
                         if (!isfinite(eta)) bad = true;
                         out0[off] = eta;
                         local_min = fminf(local_min, eta + c.D);
+                        local_max = fmaxf(local_max, eta + c.D);
                     } else {
                         // momentum update; no sponge, filter or friction in a deep tile
                         const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
@@ -667,18 +721,26 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
                 sh_c = sh_n;
             }
             if (bad) atomicOr(&ctl->errors, 1u);
-            for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
-            if (lane == 0) red[warp] = local_min;
+            for (int o = 16; o > 0; o >>= 1) {
+                local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+                if (PHASE == 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+            }
+            if (lane == 0) {
+                red[warp] = local_min;
+                if (PHASE == 1) red[DWARPS + warp] = local_max;
+            }
         }
         __syncthreads();   // every warp is done with the staged window and the row metrics
         if (d.run && threadIdx.x == 0) {
             float m = red[0];
             for (int k = 1; k < DWARPS; k++) m = fminf(m, red[k]);
             if (PHASE == 1) {
-                s.tile_hmin[p ^ 1][2 * d.tile + d.half] = m;
+                float mx = red[DWARPS];
+                for (int k = 1; k < DWARPS; k++) mx = fmaxf(mx, red[DWARPS + k]);
+                s.usum[p ^ 1][d.uidx] = make_float2(m, mx);
             } else {
                 atomicMin(&ctl->dt_bits, __float_as_uint(m));
-                if (d.half == 0) atomicAdd(&ctl->tiles_deep, 1ull);
+                atomicAdd(&ctl->units_deep, 1ull);
             }
         }
         __syncthreads();   // red[] is reused by the next unit
@@ -686,8 +748,9 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
     }
 }
 
-// General kernel: phase 0 over the whole work list, phases 1 and 2 over the
-// general list of the step.
+// General kernel, one work unit (half tile) per CTA iteration: phase 0 over
+// every unit of the work list, phases 1 and 2 over the general list of the
+// step.
 template <int PHASE>
 __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                                   const int *__restrict__ nwork_ptr, const int *__restrict__ lists,
@@ -695,17 +758,19 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
 {
     __shared__ float red[2 * WARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int nitems = (PHASE == 0) ? *nwork_ptr : lists[1];
+    const int nitems = (PHASE == 0) ? 2 * *nwork_ptr : lists[1];
     for (int g = blockIdx.x; g < nitems; g += gridDim.x) {
-        const int w = (PHASE == 0) ? g : general_items(lists, cap)[g];
-        const int2 item = work[w];
+        const int u = (PHASE == 0) ? g : general_items(lists, cap)[g];
+        const int2 item = work[u >> 1];
         const ScenarioDev &s = scen[item.x];
         ScenarioCtl *ctl = s.ctl;
         const int status = *((volatile int *)&ctl->status);
         if (PHASE != 0 && status != kRunning) continue;
         const int nx = s.nx, ny = s.ny;
         const int ty = item.y / s.tiles_x, tx = item.y - ty * s.tiles_x;
-        const int x0 = tx * kTileX + warp * OUTW, y0 = ty * TY;
+        const int uy = 2 * ty + (u & 1);
+        const int x0 = tx * kTileX + warp * OUTW, y0 = uy * kHalfRows;
+        if (y0 >= ny) continue;   // a unit below the grid (phase 0 only; never listed)
         const int p = ctl->parity;
         const float dt = (float)ctl->dt;
         const float t_sec = (float)(ctl->t * ctl->T);
@@ -713,15 +778,15 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         const int col = map_col(gx, nx, s.periodic);
         const bool has_edge = (lane >= 2) && (lane <= 30) && (gx <= nx);
         const bool has_cell = (lane >= 2) && (lane <= 29) && (gx < nx);
-        const int y_end = min(y0 + TY, ny);
+        const int y_end = min(y0 + kHalfRows, ny);
         const float *eta_in = (PHASE == 2) ? s.eta[p ^ 1] : s.eta[p];
         const float *qx_in = s.qx[p], *qy_in = s.qy[p];
         const size_t pitch = (size_t)s.pitch;
         const bool x_ghost_lo = !s.periodic && gx == 0, x_ghost_hi = !s.periodic && gx == nx;
         const bool x_nolim = (gx < 2) || (gx > nx - 2);
         const bool sponge = (s.sp_left | s.sp_right | s.sp_up | s.sp_low) != 0;
-        float local_min = FLT_MAX;    // phase 1: upper half tile's depth minimum; else dt
-        float local_min1 = FLT_MAX;   // phase 1: lower half tile's depth minimum
+        float local_min = FLT_MAX;    // phase 1: depth minimum; else dt
+        float local_max = -FLT_MAX;   // phase 1: depth maximum
         bool bad = false;
 
         if (x0 < nx) {
@@ -857,8 +922,8 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                         }
                         if (!isfinite(eta)) bad = true;
                         s.eta[p ^ 1][idx] = eta;
-                        if (yo < y0 + kHalfRows) local_min = fminf(local_min, eta + D);
-                        else local_min1 = fminf(local_min1, eta + D);
+                        local_min = fminf(local_min, eta + D);
+                        local_max = fmaxf(local_max, eta + D);
                     } else {
                         // momentum update (src/GPU/Volumen_kernel.cu:175-219)
                         const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
@@ -929,24 +994,23 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         }
         if (bad) atomicOr(&ctl->errors, 1u);
 
-        // ---- tile min: phase 1 depth -> tile_hmin (per half); phase 0/2 dt -> scenario min ----
+        // ---- unit reductions: phase 1 depth {min, max} -> usum; phase 0/2 dt -> scenario min ----
         for (int o = 16; o > 0; o >>= 1) {
             local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
-            if (PHASE == 1) local_min1 = fminf(local_min1, __shfl_xor_sync(0xffffffffu, local_min1, o));
+            if (PHASE == 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
         }
         if (lane == 0) {
             red[warp] = local_min;
-            if (PHASE == 1) red[WARPS + warp] = local_min1;
+            if (PHASE == 1) red[WARPS + warp] = local_max;
         }
         __syncthreads();
         if (threadIdx.x == 0) {
             float m = red[0];
             for (int k = 1; k < WARPS; k++) m = fminf(m, red[k]);
             if (PHASE == 1) {
-                float m1 = red[WARPS];
-                for (int k = 1; k < WARPS; k++) m1 = fminf(m1, red[WARPS + k]);
-                s.tile_hmin[p ^ 1][2 * item.y] = m;
-                s.tile_hmin[p ^ 1][2 * item.y + 1] = m1;
+                float mx = red[WARPS];
+                for (int k = 1; k < WARPS; k++) mx = fmaxf(mx, red[WARPS + k]);
+                s.usum[p ^ 1][(size_t)uy * s.tiles_x + tx] = make_float2(m, mx);
             } else {
                 atomicMin(&ctl->dt_bits, __float_as_uint(m));
             }
@@ -954,7 +1018,7 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                 // initial dt: the last tile stores the min and resets the counters
                 __threadfence();
                 const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
-                if (prev == (unsigned)(s.ntiles - 1)) {
+                if (prev == (unsigned)(s.tiles_x * units_y(s) - 1)) {
                     __threadfence();
                     ctl->dt = (double)__uint_as_float(atomicOr(&ctl->dt_bits, 0u));
                     ctl->dt_bits = 0x7f7fffffu;

@@ -63,7 +63,7 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
     size_t b = 10 * pitch * ny * sizeof(float);          // fields
     b += (size_t)(5 * ny + 1) * sizeof(float);           // row tables
     b += 3 * (size_t)nx * ny * sizeof(float);            // output staging
-    b += 4 * (size_t)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * sizeof(float);   // tile minima
+    b += 2 * (size_t)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(float2) + 1);
     b += kNumMaps * sizeof(TmaMap) + (size_t)(ny + 1) * sizeof(float4);
     if (has_faults) b += (size_t)nx * ny * sizeof(double);
     return b + 4096;
@@ -83,7 +83,8 @@ DevScenario::~DevScenario()
     cudaFree(d_gauge);
     cudaFree(d_out);
     cudaFree(fault_times_d);
-    cudaFree(hmin);
+    cudaFree(usum);
+    cudaFree(dry_age);
     cudaFree(tmaps);
     cudaFree(rowpack);
 }
@@ -177,9 +178,11 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.tiles_x = (nx + kTileX - 1) / kTileX;
     desc.tiles_y = (ny + kTileY - 1) / kTileY;
     desc.ntiles = desc.tiles_x * desc.tiles_y;
-    THY_CK(cudaMalloc(&hmin, 4 * (size_t)desc.ntiles * sizeof(float)));
-    desc.tile_hmin[0] = hmin;
-    desc.tile_hmin[1] = hmin + 2 * desc.ntiles;
+    THY_CK(cudaMalloc(&usum, 4 * (size_t)desc.ntiles * sizeof(float2)));
+    THY_CK(cudaMalloc(&dry_age, 2 * (size_t)desc.ntiles));
+    desc.usum[0] = usum;
+    desc.usum[1] = usum + 2 * desc.ntiles;
+    desc.dry_age = dry_age;
     desc.periodic = (std::fabs(p->border_left - 2.0) < 2.220446049250313e-16) &&
                     (std::fabs(p->border_right - 2.0) < 2.220446049250313e-16);
     desc.b_up = (float)p->border_up;
@@ -313,11 +316,14 @@ int DevScenario::encode_tensor_maps(cudaStream_t st)
     return THY_OK;
 }
 
-// The state changed outside phase 1: no tile counts as deep until phase 1
-// has measured the tile minima again (all-ones bytes are NaN floats).
+// The state changed outside phase 1: no unit counts as deep or dry until
+// phase 1 has measured the depth summaries again (all-ones bytes are NaN
+// floats) and the dry count starts again.
 cudaError_t DevScenario::invalidate_tile_minima(cudaStream_t st)
 {
-    return cudaMemsetAsync(hmin, 0xff, 4 * (size_t)desc.ntiles * sizeof(float), st);
+    cudaError_t e = cudaMemsetAsync(usum, 0xff, 4 * (size_t)desc.ntiles * sizeof(float2), st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dry_age, 0, 2 * (size_t)desc.ntiles, st);
+    return e;
 }
 
 int DevScenario::upload_ctl(cudaStream_t st)
@@ -458,7 +464,7 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     THY_CK(cudaMallocHost(&h_ctl, cap * sizeof(ScenarioCtl)));
     THY_CK(cudaMalloc(&d_work, std::max(max_work, 1) * sizeof(int2)));
     THY_CK(cudaMalloc(&d_nwork, sizeof(int)));
-    THY_CK(cudaMalloc(&d_lists, (2 + 2 * (size_t)std::max(max_work, 1)) * sizeof(int)));
+    THY_CK(cudaMalloc(&d_lists, (2 + 4 * (size_t)std::max(max_work, 1)) * sizeof(int)));
     THY_CK(cudaMemsetAsync(d_lists, 0, 2 * sizeof(int), st));
     THY_CK(cudaEventCreate(&ev0));
     THY_CK(cudaEventCreate(&ev1));
@@ -515,7 +521,7 @@ int Batch::rebuild()
         d_lists = nullptr;
         work_capacity = (int)work.size();
         THY_CK(cudaMalloc(&d_work, work_capacity * sizeof(int2)));
-        THY_CK(cudaMalloc(&d_lists, (2 + 2 * (size_t)work_capacity) * sizeof(int)));
+        THY_CK(cudaMalloc(&d_lists, (2 + 4 * (size_t)work_capacity) * sizeof(int)));
     }
     nwork = (int)work.size();
     THY_CK(cudaMemcpyAsync(d_table, table.data(), capacity * sizeof(ScenarioDev), cudaMemcpyHostToDevice, st));
@@ -564,11 +570,11 @@ StepLaunch Batch::params() const
     L.work = d_work;
     L.nwork = d_nwork;
     L.lists = d_lists;
-    L.cap = work_capacity;
+    L.cap = 2 * work_capacity;   // lists hold work units (two per work-list entry)
     L.grid = grid;
     L.deep_grid[0] = deep_grid[0];
     L.deep_grid[1] = deep_grid[1];
-    L.classify_grid = std::max(1, std::min((nwork + 255) / 256, 4 * device_sm_count()));
+    L.classify_grid = std::max(1, std::min((2 * nwork + 255) / 256, 4 * device_sm_count()));
     L.nslots = capacity;
     return L;
 }
@@ -737,8 +743,9 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
                 stats->kernel_launches = b.launches;
                 stats->snapshots = s.snapshots;
                 stats->series_samples = s.series;
-                stats->tiles = s.hctl.step * (long long)s.desc.ntiles;
-                stats->deep_tiles = (long long)s.hctl.tiles_deep;
+                stats->tiles = s.hctl.step * (long long)s.units();
+                stats->deep_tiles = (long long)s.hctl.units_deep;
+                stats->dry_tiles = (long long)s.hctl.units_dry;
             }
         }
         rc = s.finish(o, st);
@@ -858,11 +865,12 @@ extern "C" int thy_session_profile(thy_session *S, long long steps, double *phas
 
 extern "C" long long thy_session_launches(const thy_session *S) { return S ? S->b.launches : 0; }
 
-extern "C" int thy_session_tiles(const thy_session *S, long long *tiles, long long *deep_tiles)
+extern "C" int thy_session_tiles(const thy_session *S, long long *tiles, long long *deep_tiles, long long *dry_tiles)
 {
     if (!S) return THY_ERR_INVALID;
-    if (tiles) *tiles = S->s.hctl.step * (long long)S->s.desc.ntiles;
-    if (deep_tiles) *deep_tiles = (long long)S->s.hctl.tiles_deep;
+    if (tiles) *tiles = S->s.hctl.step * (long long)S->s.units();
+    if (deep_tiles) *deep_tiles = (long long)S->s.hctl.units_deep;
+    if (dry_tiles) *dry_tiles = (long long)S->s.hctl.units_dry;
     return THY_OK;
 }
 

@@ -44,7 +44,8 @@ struct DevScenario {
     float *d_gauge = nullptr;      // 4 floats per gauge
     float *d_out = nullptr;        // 3 planes nx*ny for snapshots / outputs
     double *fault_times_d = nullptr;
-    float *hmin = nullptr;         // 2 parities x 2 ntiles half-tile depth minima (desc.tile_hmin)
+    float2 *usum = nullptr;        // 2 parities x 2 ntiles unit depth summaries (desc.usum)
+    unsigned char *dry_age = nullptr;   // 2 ntiles (desc.dry_age)
     TmaMap *tmaps = nullptr;       // kNumMaps tensor maps of the field planes (desc.tmap)
     float4 *rowpack = nullptr;     // ny+1 packed row metrics (desc.rowpack)
     ScenarioCtl *ctl = nullptr;    // device control block (owned by the batch slot)
@@ -66,6 +67,7 @@ struct DevScenario {
     std::vector<float> ts_min, ts_max;
     double first_dt_s = 0;
 
+    long long units() const { return (long long)desc.tiles_x * ((ny + kHalfRows - 1) / kHalfRows); }   // work units
     ~DevScenario();
     int setup(const thy_problem *p, cudaStream_t st);   // allocate, upload, initial dt
     int upload_ctl(cudaStream_t st);

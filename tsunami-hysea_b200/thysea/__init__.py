@@ -144,7 +144,8 @@ def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = Tru
                          bathy=pts["series_bathy"][:pc.npoints])
     res.update(iterations=st.steps, final_time=st.final_time_s, first_dt=st.first_dt_s,
                loop_seconds=st.loop_seconds, device_ms=st.device_loop_ms, kernel_launches=st.kernel_launches,
-               nsnaps=st.snapshots, nseries=st.series_samples, tiles=st.tiles, deep_tiles=st.deep_tiles)
+               nsnaps=st.snapshots, nseries=st.series_samples, tiles=st.tiles, deep_tiles=st.deep_tiles,
+               dry_tiles=st.dry_tiles)
     return res
 
 
@@ -188,10 +189,11 @@ class Session:
         return int(_ffi.lib().thy_session_launches(self._h))
 
     def tiles(self):
-        """(phase-2 tiles stepped, of which by the deep-water kernels)"""
-        t, d = ctypes.c_longlong(), ctypes.c_longlong()
-        _check(_ffi.lib().thy_session_tiles(self._h, ctypes.byref(t), ctypes.byref(d)), "thy_session_tiles")
-        return t.value, d.value
+        """(work units x steps so far, of which deep-water, of which skipped dry land)"""
+        t, d, r = ctypes.c_longlong(), ctypes.c_longlong(), ctypes.c_longlong()
+        _check(_ffi.lib().thy_session_tiles(self._h, ctypes.byref(t), ctypes.byref(d), ctypes.byref(r)),
+               "thy_session_tiles")
+        return t.value, d.value, r.value
 
     def fetch(self):
         c = self.prep.c

@@ -67,7 +67,7 @@ class Stats(ctypes.Structure):
         ("steps", ctypes.c_longlong), ("final_time_s", ctypes.c_double), ("first_dt_s", ctypes.c_double),
         ("loop_seconds", ctypes.c_double), ("device_loop_ms", ctypes.c_double),
         ("kernel_launches", ctypes.c_longlong), ("snapshots", ctypes.c_int), ("series_samples", ctypes.c_int),
-        ("tiles", ctypes.c_longlong), ("deep_tiles", ctypes.c_longlong),
+        ("tiles", ctypes.c_longlong), ("deep_tiles", ctypes.c_longlong), ("dry_tiles", ctypes.c_longlong),
     ]
 
 
@@ -103,8 +103,8 @@ SIGNATURES = {
     "thy_session_profile": ([ctypes.c_void_p, ctypes.c_longlong, f64p, f64p], ctypes.c_int),
     "thy_session_profile_launches": ([ctypes.c_void_p, ctypes.c_longlong, f64p], ctypes.c_int),
     "thy_session_launches": ([ctypes.c_void_p], ctypes.c_longlong),
-    "thy_session_tiles": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)],
-                          ctypes.c_int),
+    "thy_session_tiles": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
+                           ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "thy_session_close": ([ctypes.c_void_p], None),
 }
 
