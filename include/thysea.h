@@ -125,6 +125,9 @@ typedef struct thy_stats {
     long long tiles;          /* work units (112 x 16-cell half tiles) x steps */
     long long deep_tiles;     /* ... stepped by the deep-water kernels (phase 2) */
     long long dry_tiles;      /* ... skipped as settled dry land */
+    double setup_seconds;     /* device set-up before the loop: upload, metrics, graph capture */
+    double output_seconds;    /* extraction and download of the output fields after the loop */
+    double total_seconds;     /* the whole call, release of the device buffers included */
 } thy_stats;
 
 /* Library / device. */
@@ -132,6 +135,10 @@ const char *thy_version(void);
 const char *thy_strerror(int code);
 int thy_device_count(void);                       /* 0 when no CUDA device is usable */
 int thy_set_device(int device);
+/* Page-lock / release caller-owned host memory (inputs of thy_problem, output
+   fields) so that thy_run's host<->device copies run at full speed. */
+int thy_host_register(void *p, size_t bytes);
+int thy_host_unregister(void *p);
 
 /* Problem set-up: file loader (problem .txt + GRD + points, the grammar of
  * src/Problema.cxx:176-343) into a raw problem owned by the library, and the

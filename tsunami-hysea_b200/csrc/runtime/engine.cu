@@ -47,6 +47,13 @@ int ensure_device()
     THY_CK(cudaSetDevice(g_device));
     if (!g_configured[g_device]) {
         THY_CK(configure_step_kernels());
+        // device buffers come from the stream-ordered default pool; freed
+        // memory stays in the pool for the next scenario instead of going
+        // back to the driver
+        cudaMemPool_t pool;
+        THY_CK(cudaDeviceGetDefaultMemPool(&pool, g_device));
+        unsigned long long keep = ~0ull;
+        THY_CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         THY_CK(cudaDeviceGetAttribute(&g_sms[g_device], cudaDevAttrMultiProcessorCount, g_device));
         g_configured[g_device] = true;
     }
@@ -75,24 +82,25 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
 
 DevScenario::~DevScenario()
 {
-    cudaFree(fields);
-    cudaFree(rows);
-    cudaFree(def);
-    cudaFree(maxbits);
-    cudaFree(d_cells);
-    cudaFree(d_gauge);
-    cudaFree(d_out);
-    cudaFree(fault_times_d);
-    cudaFree(usum);
-    cudaFree(dry_age);
-    cudaFree(tmaps);
-    cudaFree(rowpack);
+    if (fields) cudaFreeAsync(fields, ast);
+    if (rows) cudaFreeAsync(rows, ast);
+    if (def) cudaFreeAsync(def, ast);
+    if (maxbits) cudaFreeAsync(maxbits, ast);
+    if (d_cells) cudaFreeAsync(d_cells, ast);
+    if (d_gauge) cudaFreeAsync(d_gauge, ast);
+    if (d_out) cudaFreeAsync(d_out, ast);
+    if (fault_times_d) cudaFreeAsync(fault_times_d, ast);
+    if (usum) cudaFreeAsync(usum, ast);
+    if (dry_age) cudaFreeAsync(dry_age, ast);
+    if (tmaps) cudaFreeAsync(tmaps, ast);
+    if (rowpack) cudaFreeAsync(rowpack, ast);
 }
 
 int DevScenario::setup(const thy_problem *p, cudaStream_t st)
 {
     if (!p || p->nx < 2 || p->ny < 2 || !p->h || !p->Hs || !p->area_cos || !p->dlon || !p->dlat || !p->lon || !p->lat)
         return THY_ERR_INVALID;
+    ast = st;
     nx = p->nx;
     ny = p->ny;
     pitch = round_up(nx, 32);
@@ -121,21 +129,21 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
                  p->point_cell ? p->point_cell + std::max(p->npoints, 0) : nullptr);
     const int nf = (int)(faults.size() / 10);
 
-    THY_CK(cudaMalloc(&fields, 10 * plane * sizeof(float)));
-    THY_CK(cudaMalloc(&rows, (size_t)(5 * ny + 1) * sizeof(float)));
-    THY_CK(cudaMalloc(&d_out, 3 * n * sizeof(float)));
+    THY_CK(cudaMallocAsync(&fields, 10 * plane * sizeof(float), st));
+    THY_CK(cudaMallocAsync(&rows, (size_t)(5 * ny + 1) * sizeof(float), st));
+    THY_CK(cudaMallocAsync(&d_out, 3 * n * sizeof(float), st));
     if (nf > 0) {
-        THY_CK(cudaMalloc(&def, n * sizeof(double)));
-        THY_CK(cudaMalloc(&maxbits, sizeof(unsigned int)));
-        THY_CK(cudaMalloc(&fault_times_d, nf * sizeof(double)));
+        THY_CK(cudaMallocAsync(&def, n * sizeof(double), st));
+        THY_CK(cudaMallocAsync(&maxbits, sizeof(unsigned int), st));
+        THY_CK(cudaMallocAsync(&fault_times_d, nf * sizeof(double), st));
         std::vector<double> tf(nf);
         for (int i = 0; i < nf; i++) tf[i] = faults[10 * i];
         THY_CK(cudaMemcpyAsync(fault_times_d, tf.data(), nf * sizeof(double), cudaMemcpyHostToDevice, st));
         THY_CK(cudaStreamSynchronize(st));
     }
     if (!cells.empty()) {
-        THY_CK(cudaMalloc(&d_cells, cells.size() * sizeof(int)));
-        THY_CK(cudaMalloc(&d_gauge, 4 * cells.size() * sizeof(float)));
+        THY_CK(cudaMallocAsync(&d_cells, cells.size() * sizeof(int), st));
+        THY_CK(cudaMallocAsync(&d_gauge, 4 * cells.size() * sizeof(float), st));
         THY_CK(cudaMemcpyAsync(d_cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice, st));
         ts_min.assign(cells.size(), 1e30f);
         ts_max.assign(cells.size(), -1e30f);
@@ -160,7 +168,7 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
             const bool cell = y < ny;
             pk[y] = make_float4(cell ? cosr[y] : 1.f, cell ? ilc[y] : 0.f, cell ? ar[y] : 1.f, dlo[y]);
         }
-        THY_CK(cudaMalloc(&rowpack, pk.size() * sizeof(float4)));
+        THY_CK(cudaMallocAsync(&rowpack, pk.size() * sizeof(float4), st));
         THY_CK(cudaMemcpyAsync(rows, r.data(), r.size() * sizeof(float), cudaMemcpyHostToDevice, st));
         THY_CK(cudaMemcpyAsync(rowpack, pk.data(), pk.size() * sizeof(float4), cudaMemcpyHostToDevice, st));
         THY_CK(cudaStreamSynchronize(st));
@@ -178,8 +186,8 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.tiles_x = (nx + kTileX - 1) / kTileX;
     desc.tiles_y = (ny + kTileY - 1) / kTileY;
     desc.ntiles = desc.tiles_x * desc.tiles_y;
-    THY_CK(cudaMalloc(&usum, 4 * (size_t)desc.ntiles * sizeof(float2)));
-    THY_CK(cudaMalloc(&dry_age, 2 * (size_t)desc.ntiles));
+    THY_CK(cudaMallocAsync(&usum, 4 * (size_t)desc.ntiles * sizeof(float2), st));
+    THY_CK(cudaMallocAsync(&dry_age, 2 * (size_t)desc.ntiles, st));
     desc.usum[0] = usum;
     desc.usum[1] = usum + 2 * desc.ntiles;
     desc.dry_age = dry_age;
@@ -217,7 +225,7 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     {
         double *tmp = nullptr;
         const bool hasq = p->qx && p->qy;
-        THY_CK(cudaMalloc(&tmp, (hasq ? 4 : 2) * n * sizeof(double)));
+        THY_CK(cudaMallocAsync(&tmp, (hasq ? 4 : 2) * n * sizeof(double), st));
         THY_CK(cudaMemcpyAsync(tmp, p->h, n * sizeof(double), cudaMemcpyHostToDevice, st));
         THY_CK(cudaMemcpyAsync(tmp + n, p->Hs, n * sizeof(double), cudaMemcpyHostToDevice, st));
         if (hasq) {
@@ -228,7 +236,7 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
         THY_CK(cudaGetLastError());
         THY_CK(invalidate_tile_minima(st));
         THY_CK(cudaStreamSynchronize(st));
-        cudaFree(tmp);
+        cudaFreeAsync(tmp, st);
     }
 
     std::memset(&hctl, 0, sizeof(hctl));
@@ -309,7 +317,7 @@ int DevScenario::encode_tensor_maps(cudaStream_t st)
             return THY_ERR_CUDA;
         }
     }
-    THY_CK(cudaMalloc(&tmaps, kNumMaps * sizeof(TmaMap)));
+    THY_CK(cudaMallocAsync(&tmaps, kNumMaps * sizeof(TmaMap), st));
     THY_CK(cudaMemcpyAsync(tmaps, h, kNumMaps * sizeof(TmaMap), cudaMemcpyHostToDevice, st));
     THY_CK(cudaStreamSynchronize(st));
     desc.tmap = tmaps;
@@ -441,11 +449,11 @@ int DevScenario::finish(const thy_outputs *o, cudaStream_t st)
 Batch::~Batch()
 {
     if (gexec) cudaGraphExecDestroy(gexec);
-    cudaFree(d_table);
-    cudaFree(d_work);
-    cudaFree(d_nwork);
-    cudaFree(d_lists);
-    cudaFree(d_ctl);
+    if (d_table) cudaFreeAsync(d_table, st);
+    if (d_work) cudaFreeAsync(d_work, st);
+    if (d_nwork) cudaFreeAsync(d_nwork, st);
+    if (d_lists) cudaFreeAsync(d_lists, st);
+    if (d_ctl) cudaFreeAsync(d_ctl, st);
     cudaFreeHost(h_ctl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
@@ -459,12 +467,12 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     capacity = cap;
     work_capacity = max_work;
     st = stream;
-    THY_CK(cudaMalloc(&d_table, cap * sizeof(ScenarioDev)));
-    THY_CK(cudaMalloc(&d_ctl, cap * sizeof(ScenarioCtl)));
+    THY_CK(cudaMallocAsync(&d_table, cap * sizeof(ScenarioDev), st));
+    THY_CK(cudaMallocAsync(&d_ctl, cap * sizeof(ScenarioCtl), st));
     THY_CK(cudaMallocHost(&h_ctl, cap * sizeof(ScenarioCtl)));
-    THY_CK(cudaMalloc(&d_work, std::max(max_work, 1) * sizeof(int2)));
-    THY_CK(cudaMalloc(&d_nwork, sizeof(int)));
-    THY_CK(cudaMalloc(&d_lists, (2 + 4 * (size_t)std::max(max_work, 1)) * sizeof(int)));
+    THY_CK(cudaMallocAsync(&d_work, std::max(max_work, 1) * sizeof(int2), st));
+    THY_CK(cudaMallocAsync(&d_nwork, sizeof(int), st));
+    THY_CK(cudaMallocAsync(&d_lists, (2 + 4 * (size_t)std::max(max_work, 1)) * sizeof(int), st));
     THY_CK(cudaMemsetAsync(d_lists, 0, 2 * sizeof(int), st));
     THY_CK(cudaEventCreate(&ev0));
     THY_CK(cudaEventCreate(&ev1));
@@ -516,12 +524,12 @@ int Batch::rebuild()
         for (int t = 0; t < members[i]->desc.ntiles; t++) work.push_back(make_int2(i, t));
     }
     if ((int)work.size() > work_capacity) {
-        cudaFree(d_work);
-        cudaFree(d_lists);
+        cudaFreeAsync(d_work, st);
+        cudaFreeAsync(d_lists, st);
         d_lists = nullptr;
         work_capacity = (int)work.size();
-        THY_CK(cudaMalloc(&d_work, work_capacity * sizeof(int2)));
-        THY_CK(cudaMalloc(&d_lists, (2 + 4 * (size_t)work_capacity) * sizeof(int)));
+        THY_CK(cudaMallocAsync(&d_work, work_capacity * sizeof(int2), st));
+        THY_CK(cudaMallocAsync(&d_lists, (2 + 4 * (size_t)work_capacity) * sizeof(int), st));
     }
     nwork = (int)work.size();
     THY_CK(cudaMemcpyAsync(d_table, table.data(), capacity * sizeof(ScenarioDev), cudaMemcpyHostToDevice, st));
@@ -693,6 +701,25 @@ extern "C" int thy_device_count(void)
     return n;
 }
 
+// Page-locks (and releases) host memory the caller owns, e.g. the problem's
+// FP64 arrays and the output fields, so that the copies of thy_run run at
+// full link speed.
+extern "C" int thy_host_register(void *p, size_t bytes)
+{
+    int rc = ensure_device();
+    if (rc) return rc;
+    if (!p || bytes == 0) return THY_ERR_INVALID;
+    THY_CK(cudaHostRegister(p, bytes, cudaHostRegisterDefault));
+    return THY_OK;
+}
+
+extern "C" int thy_host_unregister(void *p)
+{
+    if (!p) return THY_ERR_INVALID;
+    THY_CK(cudaHostUnregister(p));
+    return THY_OK;
+}
+
 extern "C" int thy_set_device(int device)
 {
     if (device < 0 || device >= 64) return THY_ERR_INVALID;
@@ -705,6 +732,7 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
     int rc = ensure_device();
     if (rc) return rc;
     if (!p) return THY_ERR_INVALID;
+    const auto t_start = std::chrono::steady_clock::now();
     cudaStream_t st;
     THY_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     auto t0 = std::chrono::steady_clock::now();
@@ -717,6 +745,7 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
         s.desc.ctl = s.ctl;
         if ((rc = b.rebuild())) goto out;
         t0 = std::chrono::steady_clock::now();
+        if (stats) stats->setup_seconds = std::chrono::duration<double>(t0 - t_start).count();
         if ((rc = initial_dt(b))) goto out;
         for (;;) {
             if (!(s.hctl.t < s.t_end)) break;
@@ -748,10 +777,16 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
                 stats->dry_tiles = (long long)s.hctl.units_dry;
             }
         }
-        rc = s.finish(o, st);
+        {
+            const auto t2 = std::chrono::steady_clock::now();
+            rc = s.finish(o, st);
+            if (stats)
+                stats->output_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t2).count();
+        }
     out:;
     }
     cudaStreamDestroy(st);
+    if (stats) stats->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
     return rc;
 }
 

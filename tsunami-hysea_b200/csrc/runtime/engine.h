@@ -49,6 +49,7 @@ struct DevScenario {
     TmaMap *tmaps = nullptr;       // kNumMaps tensor maps of the field planes (desc.tmap)
     float4 *rowpack = nullptr;     // ny+1 packed row metrics (desc.rowpack)
     ScenarioCtl *ctl = nullptr;    // device control block (owned by the batch slot)
+    cudaStream_t ast = nullptr;    // stream the buffers were allocated on (stream-ordered pool)
     ScenarioDev desc{};            // descriptor (device pointers), host copy
     // problem data kept on the host
     double Hs = 1, Qs = 1, Ts = 1, Hmin = 0, Ls = 1;

@@ -92,22 +92,78 @@ class Prepared:
     def npoints(self) -> int:
         return int(self.c.npoints)
 
+    def pin(self):
+        """Page-locks the problem's FP64 cell arrays (h, Hs, qx, qy) so that
+        every thy_run uploads them at full link speed."""
+        if getattr(self, "_pinned", None):
+            return self
+        L, c = _ffi.lib(), self.c
+        n = int(c.nx) * int(c.ny)
+        self._pinned = []
+        for name in ("h", "Hs", "qx", "qy"):
+            ptr = ctypes.cast(getattr(c, name), ctypes.c_void_p)
+            if ptr.value:
+                _check(L.thy_host_register(ptr, n * 8), "thy_host_register")
+                self._pinned.append(ptr)
+        return self
+
     def __del__(self):
         try:
+            for ptr in getattr(self, "_pinned", None) or []:
+                _ffi.lib().thy_host_unregister(ptr)
             if getattr(self, "_h", None):
                 _ffi.lib().thy_problem_free(self._h)
         except Exception:
             pass
 
 
-def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = True) -> Dict:
-    """Runs one scenario end to end on the GPU through thy_run()."""
+OUTPUT_FIELDS = ("max_height", "arrival", "deformed_bathy", "eta", "ux", "uy")
+
+
+class PinnedOutputs:
+    """Page-locked output fields for repeated runs of one grid (thysea.run's
+    `out`): allocated and registered once, reused by every run."""
+
+    def __init__(self, prep: "Prepared"):
+        ny, nx = int(prep.c.ny), int(prep.c.nx)
+        self.fields = {k: np.empty((ny, nx), np.float32) for k in OUTPUT_FIELDS}
+        L = _ffi.lib()
+        self._reg = []
+        for v in self.fields.values():
+            v.fill(0)   # touch the pages before locking them
+            ptr = ctypes.c_void_p(v.ctypes.data)
+            _check(L.thy_host_register(ptr, v.nbytes), "thy_host_register")
+            self._reg.append(ptr)
+
+    def release(self):
+        for ptr in self._reg:
+            _ffi.lib().thy_host_unregister(ptr)
+        self._reg = []
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass
+
+
+def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = True,
+        out: Optional[Dict[str, np.ndarray]] = None) -> Dict:
+    """Runs one scenario end to end on the GPU through thy_run().  `out`:
+    caller-owned (ny, nx) float32 output fields to fill (e.g.
+    PinnedOutputs.fields); new arrays otherwise."""
     L = _ffi.lib()
     prep = problem if isinstance(problem, Prepared) else Prepared(problem)
     pc = prep.c
     pc.max_steps = max_steps
     ny, nx = pc.ny, pc.nx
-    fields = {k: np.empty((ny, nx), np.float32) for k in ("max_height", "arrival", "deformed_bathy", "eta", "ux", "uy")}
+    if out is not None:
+        fields = {k: out[k] for k in OUTPUT_FIELDS}
+        for v in fields.values():
+            if v.shape != (ny, nx) or v.dtype != np.float32 or not v.flags.c_contiguous:
+                raise ValueError("output fields must be C-contiguous float32 arrays of shape (ny, nx)")
+    else:
+        fields = {k: np.empty((ny, nx), np.float32) for k in OUTPUT_FIELDS}
     npts = max(pc.npoints, 1)
     pts = {k: np.empty(npts, np.float32) for k in ("series_min", "series_max", "series_bathy")}
     snaps = {"time": [], "eta": [], "ux": [], "uy": []}
@@ -145,7 +201,8 @@ def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = Tru
     res.update(iterations=st.steps, final_time=st.final_time_s, first_dt=st.first_dt_s,
                loop_seconds=st.loop_seconds, device_ms=st.device_loop_ms, kernel_launches=st.kernel_launches,
                nsnaps=st.snapshots, nseries=st.series_samples, tiles=st.tiles, deep_tiles=st.deep_tiles,
-               dry_tiles=st.dry_tiles)
+               dry_tiles=st.dry_tiles, setup_seconds=st.setup_seconds, output_seconds=st.output_seconds,
+               total_seconds=st.total_seconds)
     return res
 
 

@@ -68,6 +68,7 @@ class Stats(ctypes.Structure):
         ("loop_seconds", ctypes.c_double), ("device_loop_ms", ctypes.c_double),
         ("kernel_launches", ctypes.c_longlong), ("snapshots", ctypes.c_int), ("series_samples", ctypes.c_int),
         ("tiles", ctypes.c_longlong), ("deep_tiles", ctypes.c_longlong), ("dry_tiles", ctypes.c_longlong),
+        ("setup_seconds", ctypes.c_double), ("output_seconds", ctypes.c_double), ("total_seconds", ctypes.c_double),
     ]
 
 
@@ -77,6 +78,8 @@ SIGNATURES = {
     "thy_strerror": ([ctypes.c_int], ctypes.c_char_p),
     "thy_device_count": ([], ctypes.c_int),
     "thy_set_device": ([ctypes.c_int], ctypes.c_int),
+    "thy_host_register": ([ctypes.c_void_p, ctypes.c_size_t], ctypes.c_int),
+    "thy_host_unregister": ([ctypes.c_void_p], ctypes.c_int),
     "thy_load_problem_file": ([ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "thy_raw_view": ([ctypes.c_void_p], ctypes.POINTER(Raw)),
     "thy_raw_name": ([ctypes.c_void_p], ctypes.c_char_p),
