@@ -84,6 +84,15 @@ constexpr int kHalfRows = 16;                 // rows of a half tile
 constexpr int kStageW = 120;                  // staged columns: x0-4 .. x0+115 (16-byte aligned start)
 constexpr int kStageRows = kHalfRows + 2;     // staged rows: one above and one below the half tile
 
+// Depth summary of a work unit for one state: {min, max} of eta + dep over
+// the unit, over its two-cell border strips (left, right, top, bottom: the
+// unit's first / last two columns or rows inside the grid) and over its four
+// 2 x 2 corners - exactly the cells the two-cell stencil ring of a
+// neighbouring unit reaches into.
+struct UnitSum {
+    float2 all, L, R, T, B, TL, TR, BL, BR;
+};
+
 struct ScenarioDev {
     int nx, ny, pitch;
     int tiles_x, tiles_y, ntiles;
@@ -100,10 +109,9 @@ struct ScenarioDev {
     float *arr;
     float *eta_ini;
     // per work unit (half tile of kTileX x kHalfRows cells; unit (tx, uy) at
-    // uy * tiles_x + tx): {min, max} of the water depth eta + dep over its
-    // cells, written by phase 1 for the state it produces (index parity^1);
-    // NaN = unknown
-    float2 *usum[2];
+    // uy * tiles_x + tx): depth summary of the state phase 1 produces (index
+    // parity^1); NaN = unknown
+    UnitSum *usum[2];
     // per unit: consecutive classifications that found its 3 x 3 unit
     // neighbourhood dry (saturating)
     unsigned char *dry_age;

@@ -263,39 +263,38 @@ __device__ __forceinline__ void y_edge(const ScenarioDev &s, const Cell &m, cons
 // ---------------------------------------------------------------------------
 // Work units and their classes.  A unit is a half tile (kTileX x kHalfRows
 // cells); work-list entry w (scenario, tile) holds units 2w (upper half) and
-// 2w+1 (lower half).  Phase 1 records each unit's depth {min, max}; from
-// those of the 3 x 3 units around (which cover the two-cell stencil ring),
-//   deep:  every cell of the neighbourhood deeper than hpos, and the unit at
+// 2w+1 (lower half).  Phase 1 records each unit's depth summary (UnitSum);
+// from the unit's own cells and the border strips and corners of its eight
+// neighbours - exactly its two-cell stencil ring -
+//   deep:  every cell of unit and ring deeper than hpos, and the unit at
 //          least two cells from the boundaries and outside the sponge
 //          layers - every edge is a pure 2s edge and no cell is dried,
 //          damped or relaxed;
-//   dry:   every cell of the neighbourhood dry (depth 0) at three
-//          consecutive classifications - then both state buffers hold the
-//          scheme's fixed point (eta = -dep, q = 0), which a step would write
-//          again, so the unit is skipped;
+//   dry:   every cell of unit and ring dry (depth 0) at three consecutive
+//          classifications - then both state buffers hold the scheme's
+//          fixed point (eta = -dep, q = 0), which a step would write again,
+//          so the unit is skipped;
 //   general: the rest.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ int units_y(const ScenarioDev &s) { return (s.ny + kHalfRows - 1) / kHalfRows; }
 
 // The geometric tests imply 1 <= tx <= tiles_x - 2 and 1 <= uy <= units_y - 2.
-__device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const float2 *__restrict__ sum, int tx, int uy)
+__device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const UnitSum *__restrict__ sum, int tx, int uy)
 {
     if (!s.tmap) return false;
     const int x0 = tx * kTileX, yb = uy * kHalfRows;
     if (x0 < max(2, s.sp_left) || x0 + kTileX > s.nx - max(2, s.sp_right)) return false;
     if (yb < max(2, s.sp_up) || yb + kHalfRows > s.ny - max(2, s.sp_low)) return false;
+    const int W = s.tiles_x;
+    const UnitSum *c = sum + (size_t)uy * W + tx;
     const float hp = s.hpos;
-    bool ok = true;
-    for (int dy = -1; dy <= 1; dy++) {
-        const float2 *r = sum + (size_t)(uy + dy) * s.tiles_x + tx;
-        ok = ok && (r[-1].x > hp) && (r[0].x > hp) && (r[1].x > hp);
-    }
-    return ok;
+    return (c->all.x > hp) && (c[-1].R.x > hp) && (c[1].L.x > hp) && (c[-W].B.x > hp) && (c[W].T.x > hp) &&
+           (c[-W - 1].BR.x > hp) && (c[-W + 1].BL.x > hp) && (c[W - 1].TR.x > hp) && (c[W + 1].TL.x > hp);
 }
 
 // Outside the grid counts as dry (ghost cells copy the boundary cell), except
 // across a periodic x boundary, where the wrapped unit counts.
-__device__ __forceinline__ bool unit_dry(const ScenarioDev &s, const float2 *__restrict__ sum, int tx, int uy)
+__device__ __forceinline__ bool unit_dry(const ScenarioDev &s, const UnitSum *__restrict__ sum, int tx, int uy)
 {
     const int ny_u = units_y(s), nx_u = s.tiles_x;
     bool dry = true;
@@ -308,10 +307,88 @@ __device__ __forceinline__ bool unit_dry(const ScenarioDev &s, const float2 *__r
                 if (!s.periodic) continue;
                 x = (x + nx_u) % nx_u;
             }
-            dry = dry && (sum[(size_t)y * nx_u + x].y <= 0.f);
+            const UnitSum &u = sum[(size_t)y * nx_u + x];
+            // the part of neighbour (dx, dy) inside the ring
+            const float2 v = (dx == 0 && dy == 0) ? u.all
+                           : (dy == 0) ? (dx < 0 ? u.R : u.L)
+                           : (dx == 0) ? (dy < 0 ? u.B : u.T)
+                           : (dy < 0) ? (dx < 0 ? u.BR : u.BL)
+                                      : (dx < 0 ? u.TR : u.TL);
+            dry = dry && (v.y <= 0.f);
         }
     }
     return dry;
+}
+
+// Per-lane depth accumulators of a unit: every row, the unit's first two
+// rows and its last two rows.
+struct DepthAcc {
+    float amin, amax, tmin, tmax, bmin, bmax;
+    __device__ __forceinline__ void init()
+    {
+        amin = tmin = bmin = FLT_MAX;
+        amax = tmax = bmax = -FLT_MAX;
+    }
+    __device__ __forceinline__ void add(float h, bool top, bool bot)
+    {
+        amin = fminf(amin, h);
+        amax = fmaxf(amax, h);
+        if (top) { tmin = fminf(tmin, h); tmax = fmaxf(tmax, h); }
+        if (bot) { bmin = fminf(bmin, h); bmax = fmaxf(bmax, h); }
+    }
+};
+
+// {min, max} over the lanes of a warp that are members
+__device__ __forceinline__ float2 warp_minmax(float mn, float mx, bool member)
+{
+    if (!member) {
+        mn = FLT_MAX;
+        mx = -FLT_MAX;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        mn = fminf(mn, __shfl_xor_sync(0xffffffffu, mn, o));
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+    }
+    return make_float2(mn, mx);
+}
+
+// The nine {min, max} of one warp for the unit summary: lanes in the unit's
+// first two / last two columns (is_l / is_r); every field of a warp without
+// such cells is the empty value.  Written to slot[0..8] in UnitSum order.
+__device__ __forceinline__ void warp_unit_summary(const DepthAcc &a, bool cell, bool is_l, bool is_r, float2 *slot)
+{
+    // rows / columns a warp holds no cell of are skipped (warp-uniform tests)
+    const float2 none = make_float2(FLT_MAX, -FLT_MAX);
+    const bool has_t = __any_sync(0xffffffffu, cell && a.tmin != FLT_MAX);
+    const bool has_b = __any_sync(0xffffffffu, cell && a.bmin != FLT_MAX);
+    const bool has_l = __any_sync(0xffffffffu, is_l), has_r = __any_sync(0xffffffffu, is_r);
+    const float2 all = warp_minmax(a.amin, a.amax, cell);
+    const float2 top = has_t ? warp_minmax(a.tmin, a.tmax, cell) : none;
+    const float2 bot = has_b ? warp_minmax(a.bmin, a.bmax, cell) : none;
+    const float2 L = has_l ? warp_minmax(a.amin, a.amax, is_l) : none;
+    const float2 R = has_r ? warp_minmax(a.amin, a.amax, is_r) : none;
+    const float2 TL = (has_l && has_t) ? warp_minmax(a.tmin, a.tmax, is_l) : none;
+    const float2 TR = (has_r && has_t) ? warp_minmax(a.tmin, a.tmax, is_r) : none;
+    const float2 BL = (has_l && has_b) ? warp_minmax(a.bmin, a.bmax, is_l) : none;
+    const float2 BR = (has_r && has_b) ? warp_minmax(a.bmin, a.bmax, is_r) : none;
+    if ((threadIdx.x & 31) == 0) {
+        slot[0] = all; slot[1] = L; slot[2] = R; slot[3] = top; slot[4] = bot;
+        slot[5] = TL; slot[6] = TR; slot[7] = BL; slot[8] = BR;
+    }
+}
+
+// Combines the per-warp slots (nw warps, 9 float2 each, UnitSum order) into
+// the unit summary: thread t < 18 reduces float t (a field's min or max).
+__device__ __forceinline__ void store_unit_summary(UnitSum *dst, const float2 *slots, int nw)
+{
+    static_assert(sizeof(UnitSum) == 18 * sizeof(float), "UnitSum is 9 float2");
+    const int t = threadIdx.x;
+    if (t < 18) {
+        const float *v = reinterpret_cast<const float *>(slots) + t;
+        float r = v[0];
+        for (int w = 1; w < nw; w++) r = (t & 1) ? fmaxf(r, v[18 * w]) : fminf(r, v[18 * w]);
+        reinterpret_cast<float *>(dst)[t] = r;
+    }
 }
 
 constexpr int kDryAge = 3;   // classifications a unit must stay dry before it is skipped
@@ -444,7 +521,7 @@ __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2
                 ScenarioCtl *ctl = s.ctl;
                 const bool running = ctl->status == kRunning;
                 const int par = running ? (ctl->parity ^ 1) : ctl->parity;
-                const float2 *sum = s.usum[par];
+                const UnitSum *sum = s.usum[par];
                 deep = unit_deep(s, sum, tx, uy);
                 const size_t k = (size_t)uy * s.tiles_x + tx;
                 int age = s.dry_age[k];
@@ -563,7 +640,7 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
     // staging buffer b at dsm + b * SB
     uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + deep_misc_offset(PHASE));
     DeepRow *rows = reinterpret_cast<DeepRow *>(dsm + deep_misc_offset(PHASE) + 16);
-    float *red = reinterpret_cast<float *>(rows + kStageRows);
+    float *red = reinterpret_cast<float *>(rows + kStageRows);   // per warp: dt, or depth min and max
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int strip = warp & 3, group = warp >> 2;
     const int nunits = lists[0];
@@ -735,9 +812,13 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
             float m = red[0];
             for (int k = 1; k < DWARPS; k++) m = fminf(m, red[k]);
             if (PHASE == 1) {
+                // a deep unit reports its whole-unit {min, max} for its strips
+                // and corners too: conservative for a neighbour's deep test,
+                // and a wet unit fails a neighbour's dry test either way
                 float mx = red[DWARPS];
                 for (int k = 1; k < DWARPS; k++) mx = fmaxf(mx, red[DWARPS + k]);
-                s.usum[p ^ 1][d.uidx] = make_float2(m, mx);
+                const float2 v = make_float2(m, mx);
+                s.usum[p ^ 1][d.uidx] = UnitSum{v, v, v, v, v, v, v, v, v};
             } else {
                 atomicMin(&ctl->dt_bits, __float_as_uint(m));
                 atomicAdd(&ctl->units_deep, 1ull);
@@ -756,7 +837,8 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                                                   const int *__restrict__ nwork_ptr, const int *__restrict__ lists,
                                                   int cap)
 {
-    __shared__ float red[2 * WARPS];
+    __shared__ float red[WARPS];          // phases 0 / 2: dt per warp
+    __shared__ float2 slots[9 * WARPS];   // phase 1: unit summary per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int nitems = (PHASE == 0) ? 2 * *nwork_ptr : lists[1];
     for (int g = blockIdx.x; g < nitems; g += gridDim.x) {
@@ -785,8 +867,9 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         const bool x_ghost_lo = !s.periodic && gx == 0, x_ghost_hi = !s.periodic && gx == nx;
         const bool x_nolim = (gx < 2) || (gx > nx - 2);
         const bool sponge = (s.sp_left | s.sp_right | s.sp_up | s.sp_low) != 0;
-        float local_min = FLT_MAX;    // phase 1: depth minimum; else dt
-        float local_max = -FLT_MAX;   // phase 1: depth maximum
+        float local_min = FLT_MAX;    // phases 0 / 2: dt
+        DepthAcc hacc;                // phase 1: depth summary
+        hacc.init();
         bool bad = false;
 
         if (x0 < nx) {
@@ -922,8 +1005,7 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                         }
                         if (!isfinite(eta)) bad = true;
                         s.eta[p ^ 1][idx] = eta;
-                        local_min = fminf(local_min, eta + D);
-                        local_max = fmaxf(local_max, eta + D);
+                        hacc.add(eta + D, yo - y0 < 2, y_end - yo <= 2);
                     } else {
                         // momentum update (src/GPU/Volumen_kernel.cu:175-219)
                         const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
@@ -994,26 +1076,22 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         }
         if (bad) atomicOr(&ctl->errors, 1u);
 
-        // ---- unit reductions: phase 1 depth {min, max} -> usum; phase 0/2 dt -> scenario min ----
-        for (int o = 16; o > 0; o >>= 1) {
-            local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
-            if (PHASE == 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
-        }
-        if (lane == 0) {
-            red[warp] = local_min;
-            if (PHASE == 1) red[WARPS + warp] = local_max;
+        // ---- unit reductions: phase 1 depth summary -> usum; phase 0/2 dt -> scenario min ----
+        if (PHASE == 1) {
+            // the unit's first two and last two columns inside the grid
+            const int ux0 = tx * kTileX, ux1 = min(ux0 + kTileX, nx);
+            const bool cell = has_cell && x0 < nx;
+            warp_unit_summary(hacc, cell, cell && gx < ux0 + 2, cell && gx >= ux1 - 2, slots + 9 * warp);
+        } else {
+            for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+            if (lane == 0) red[warp] = local_min;
         }
         __syncthreads();
-        if (threadIdx.x == 0) {
+        if (PHASE == 1) store_unit_summary(&s.usum[p ^ 1][(size_t)uy * s.tiles_x + tx], slots, WARPS);
+        if (PHASE != 1 && threadIdx.x == 0) {
             float m = red[0];
             for (int k = 1; k < WARPS; k++) m = fminf(m, red[k]);
-            if (PHASE == 1) {
-                float mx = red[WARPS];
-                for (int k = 1; k < WARPS; k++) mx = fmaxf(mx, red[WARPS + k]);
-                s.usum[p ^ 1][(size_t)uy * s.tiles_x + tx] = make_float2(m, mx);
-            } else {
-                atomicMin(&ctl->dt_bits, __float_as_uint(m));
-            }
+            atomicMin(&ctl->dt_bits, __float_as_uint(m));
             if (PHASE == 0) {
                 // initial dt: the last tile stores the min and resets the counters
                 __threadfence();

@@ -70,7 +70,7 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
     size_t b = 10 * pitch * ny * sizeof(float);          // fields
     b += (size_t)(5 * ny + 1) * sizeof(float);           // row tables
     b += 3 * (size_t)nx * ny * sizeof(float);            // output staging
-    b += 2 * (size_t)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(float2) + 1);
+    b += 2 * (size_t)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(UnitSum) + 1);
     b += kNumMaps * sizeof(TmaMap) + (size_t)(ny + 1) * sizeof(float4);
     if (has_faults) b += (size_t)nx * ny * sizeof(double);
     return b + 4096;
@@ -186,7 +186,7 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.tiles_x = (nx + kTileX - 1) / kTileX;
     desc.tiles_y = (ny + kTileY - 1) / kTileY;
     desc.ntiles = desc.tiles_x * desc.tiles_y;
-    THY_CK(cudaMallocAsync(&usum, 4 * (size_t)desc.ntiles * sizeof(float2), st));
+    THY_CK(cudaMallocAsync(&usum, 4 * (size_t)desc.ntiles * sizeof(UnitSum), st));
     THY_CK(cudaMallocAsync(&dry_age, 2 * (size_t)desc.ntiles, st));
     desc.usum[0] = usum;
     desc.usum[1] = usum + 2 * desc.ntiles;
@@ -329,7 +329,7 @@ int DevScenario::encode_tensor_maps(cudaStream_t st)
 // floats) and the dry count starts again.
 cudaError_t DevScenario::invalidate_tile_minima(cudaStream_t st)
 {
-    cudaError_t e = cudaMemsetAsync(usum, 0xff, 4 * (size_t)desc.ntiles * sizeof(float2), st);
+    cudaError_t e = cudaMemsetAsync(usum, 0xff, 4 * (size_t)desc.ntiles * sizeof(UnitSum), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(dry_age, 0, 2 * (size_t)desc.ntiles, st);
     return e;
 }

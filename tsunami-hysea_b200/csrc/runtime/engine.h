@@ -44,7 +44,7 @@ struct DevScenario {
     float *d_gauge = nullptr;      // 4 floats per gauge
     float *d_out = nullptr;        // 3 planes nx*ny for snapshots / outputs
     double *fault_times_d = nullptr;
-    float2 *usum = nullptr;        // 2 parities x 2 ntiles unit depth summaries (desc.usum)
+    UnitSum *usum = nullptr;       // 2 parities x 2 ntiles unit depth summaries (desc.usum)
     unsigned char *dry_age = nullptr;   // 2 ntiles (desc.dry_age)
     TmaMap *tmaps = nullptr;       // kNumMaps tensor maps of the field planes (desc.tmap)
     float4 *rowpack = nullptr;     // ny+1 packed row metrics (desc.rowpack)
