@@ -212,6 +212,46 @@ int thy_session_tiles(const thy_session *s, long long *tiles, long long *deep_ti
 double thy_session_time(const thy_session *s);    /* simulated time (s) */
 void thy_session_close(thy_session *s);
 
+/* Multi-scenario runtime (batched and serving use): scenarios submitted at
+   any time are admitted in order under an HBM budget and stepped together -
+   one work list over all their tiles, one CUDA graph per chunk of steps -
+   and retired as they finish, each with its own dt, time and events.  A
+   scenario's results are identical alone (thy_run) and in any mix.  A
+   scenario whose state turns non-finite is retired with THY_ERR_NONFINITE
+   while the others continue. */
+typedef struct thy_server thy_server;
+typedef struct thy_server_opts {
+    long long hbm_budget_bytes;   /* device memory for scenario state (0: 90 % of the free memory) */
+    int max_scenarios;            /* scenarios stepped at once (0: 256) */
+    int device;
+} thy_server_opts;
+typedef struct thy_server_stats {
+    long long submitted, admitted, completed, failed, cancelled, rejected;
+    long long chunks;             /* graph launches */
+    int queued, running;
+    long long hbm_in_use, hbm_budget;
+    double device_ms;             /* device time of the chunks */
+    double cell_updates;          /* of retired scenarios */
+} thy_server_stats;
+/* completion callback, from thy_server_progress / drain / cancel / close:
+   status THY_OK, THY_ERR_NONFINITE, THY_ERR_CANCELLED or a set-up error;
+   stats may be NULL for a request that never ran.  For the request's
+   thy_stats: setup_seconds = time queued, loop_seconds = time admitted,
+   total_seconds = submission to result. */
+typedef void (*thy_done_fn)(void *user, long long request, int status, const thy_stats *stats);
+int thy_server_open(const thy_server_opts *opts, thy_server **out);
+/* queues a request; `p` and `o` must stay valid until its callback (nothing
+   is copied before admission); THY_ERR_BUDGET if it can never fit */
+int thy_server_submit(thy_server *s, const thy_problem *p, const thy_outputs *o, thy_done_fn done, void *user,
+                      long long *request);
+int thy_server_cancel(thy_server *s, long long request);   /* queued: now; running: at the next progress */
+/* admits, performs due events, runs one chunk of steps for every running
+   scenario and retires the finished ones; *active = queued + running */
+int thy_server_progress(thy_server *s, int *active);
+int thy_server_drain(thy_server *s);                        /* progress until nothing is queued or running */
+int thy_server_get_stats(const thy_server *s, thy_server_stats *out);
+void thy_server_close(thy_server *s);                       /* cancels what is left */
+
 #ifdef __cplusplus
 }
 #endif

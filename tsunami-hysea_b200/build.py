@@ -31,7 +31,7 @@ CUDA_SOURCES = [
     "kernels/init_extract.cu",
     "kernels/okada.cu",
     "runtime/engine.cu",
-    "runtime/batch.cu",
+    "runtime/server.cu",
     "runtime/okada_api.cu",
     "host/netcdf_out.cpp",
     "host/dropin.cpp",

@@ -452,6 +452,8 @@ Batch::~Batch()
     if (d_table) cudaFreeAsync(d_table, st);
     if (d_work) cudaFreeAsync(d_work, st);
     if (d_nwork) cudaFreeAsync(d_nwork, st);
+    if (d_work0) cudaFreeAsync(d_work0, st);
+    if (d_nwork0) cudaFreeAsync(d_nwork0, st);
     if (d_lists) cudaFreeAsync(d_lists, st);
     if (d_ctl) cudaFreeAsync(d_ctl, st);
     cudaFreeHost(h_ctl);
@@ -472,6 +474,8 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     THY_CK(cudaMallocHost(&h_ctl, cap * sizeof(ScenarioCtl)));
     THY_CK(cudaMallocAsync(&d_work, std::max(max_work, 1) * sizeof(int2), st));
     THY_CK(cudaMallocAsync(&d_nwork, sizeof(int), st));
+    THY_CK(cudaMallocAsync(&d_work0, std::max(max_work, 1) * sizeof(int2), st));
+    THY_CK(cudaMallocAsync(&d_nwork0, sizeof(int), st));
     THY_CK(cudaMallocAsync(&d_lists, (2 + 4 * (size_t)std::max(max_work, 1)) * sizeof(int), st));
     THY_CK(cudaMemsetAsync(d_lists, 0, 2 * sizeof(int), st));
     THY_CK(cudaEventCreate(&ev0));
@@ -514,7 +518,7 @@ int Batch::detach(DevScenario *s)
     return THY_OK;
 }
 
-int Batch::rebuild()
+int Batch::update()
 {
     std::vector<ScenarioDev> table(capacity);
     std::vector<int2> work;
@@ -524,23 +528,38 @@ int Batch::rebuild()
         for (int t = 0; t < members[i]->desc.ntiles; t++) work.push_back(make_int2(i, t));
     }
     if ((int)work.size() > work_capacity) {
+        // the captured graph holds the list pointers: grow, then recapture
         cudaFreeAsync(d_work, st);
+        cudaFreeAsync(d_work0, st);
         cudaFreeAsync(d_lists, st);
         d_lists = nullptr;
         work_capacity = (int)work.size();
         THY_CK(cudaMallocAsync(&d_work, work_capacity * sizeof(int2), st));
+        THY_CK(cudaMallocAsync(&d_work0, work_capacity * sizeof(int2), st));
         THY_CK(cudaMallocAsync(&d_lists, (2 + 4 * (size_t)work_capacity) * sizeof(int), st));
+        if (gexec) {
+            cudaGraphExecDestroy(gexec);
+            gexec = nullptr;
+        }
     }
     nwork = (int)work.size();
     THY_CK(cudaMemcpyAsync(d_table, table.data(), capacity * sizeof(ScenarioDev), cudaMemcpyHostToDevice, st));
     if (nwork) THY_CK(cudaMemcpyAsync(d_work, work.data(), nwork * sizeof(int2), cudaMemcpyHostToDevice, st));
     THY_CK(cudaMemcpyAsync(d_nwork, &nwork, sizeof(int), cudaMemcpyHostToDevice, st));
     THY_CK(cudaStreamSynchronize(st));
+    return reset_lists();
+}
+
+// Grids depend on the work-list capacity only, so the graph survives changes
+// of the member set (the kernels read the table and the lists from device
+// memory).
+int Batch::capture()
+{
     const int bps = std::max(1, step_blocks_per_sm());
-    grid = std::max(1, std::min(nwork, device_sm_count() * bps * 8));
+    grid = std::max(1, std::min(2 * work_capacity, device_sm_count() * bps * 8));
     for (int ph = 0; ph < 2; ph++)
-        deep_grid[ph] = std::max(1, std::min(2 * nwork, device_sm_count() * std::max(1, deep_blocks_per_sm(ph + 1))));
-    if (int rc = reset_lists()) return rc;
+        deep_grid[ph] =
+            std::max(1, std::min(2 * work_capacity, device_sm_count() * std::max(1, deep_blocks_per_sm(ph + 1))));
     if (gexec) {
         cudaGraphExecDestroy(gexec);
         gexec = nullptr;
@@ -571,6 +590,18 @@ int Batch::rebuild()
     return THY_OK;
 }
 
+int Batch::rebuild()
+{
+    int rc;
+    if (!gexec) {
+        // grids for the capture need the capacity only; lists are reset by update()
+        if ((rc = capture())) return rc;
+    }
+    if ((rc = update())) return rc;
+    if (!gexec && (rc = capture())) return rc;   // the work list grew past the capacity
+    return THY_OK;
+}
+
 StepLaunch Batch::params() const
 {
     StepLaunch L;
@@ -582,7 +613,7 @@ StepLaunch Batch::params() const
     L.grid = grid;
     L.deep_grid[0] = deep_grid[0];
     L.deep_grid[1] = deep_grid[1];
-    L.classify_grid = std::max(1, std::min((2 * nwork + 255) / 256, 4 * device_sm_count()));
+    L.classify_grid = std::max(1, std::min((2 * work_capacity + 255) / 256, 4 * device_sm_count()));
     L.nslots = capacity;
     return L;
 }
@@ -612,8 +643,31 @@ int Batch::run_chunk(bool timed)
     return THY_OK;
 }
 
+// Truncation of a member's initial dt to its first fault time
+// (src/GPU/ShallowWater.cu:382-391).
+static void truncate_initial_dt(DevScenario *s)
+{
+    double dt = s->hctl.dt, t = s->hctl.t, T = s->Ts;
+    const int nf = (int)(s->faults.size() / 10);
+    int jumping = 0;
+    if (nf > 0) {
+        const double *tf0 = &s->faults[0];
+        if (tf0[0] < 2.220446049250313e-16) {
+            int k = 1;
+            while (k < nf && !(std::fabs(s->faults[10 * k] - tf0[0]) > 2.220446049250313e-16)) k++;
+            if (k < nf && (t + dt) * T > s->faults[10 * k]) { dt = s->faults[10 * k] / T - t; jumping = 1; }
+        } else if ((t + dt) * T > tf0[0]) {
+            dt = tf0[0] / T - t;
+            jumping = 1;
+        }
+    }
+    s->hctl.dt = dt;
+    s->hctl.jumping = jumping;
+    s->first_dt_s = dt * T;
+}
+
 // Initial dt of every member (src/GPU/Timestep.cu:11-33) and the truncation
-// to the first fault time (src/GPU/ShallowWater.cu:382-391).
+// to the first fault time.
 static int initial_dt(Batch &b)
 {
     int rc;
@@ -627,32 +681,47 @@ static int initial_dt(Batch &b)
         DevScenario *s = b.members[i];
         if (!s) continue;
         s->hctl = b.h_ctl[i];
-        double dt = s->hctl.dt, t = s->hctl.t, T = s->Ts;
-        const int nf = (int)(s->faults.size() / 10);
-        int jumping = 0;
-        if (nf > 0) {
-            const double *tf0 = &s->faults[0];
-            if (tf0[0] < 2.220446049250313e-16) {
-                int k = 1;
-                while (k < nf && !(std::fabs(s->faults[10 * k] - tf0[0]) > 2.220446049250313e-16)) k++;
-                if (k < nf && (t + dt) * T > s->faults[10 * k]) { dt = s->faults[10 * k] / T - t; jumping = 1; }
-            } else if ((t + dt) * T > tf0[0]) {
-                dt = tf0[0] / T - t;
-                jumping = 1;
-            }
-        }
-        s->hctl.dt = dt;
-        s->hctl.jumping = jumping;
-        s->first_dt_s = dt * T;
+        truncate_initial_dt(s);
     }
     return THY_OK;
 }
 
-// Host side of one loop iteration's events (src/GPU/ShallowWater.cu:398-421).
-static int handle_events(DevScenario &s, const thy_outputs *o, cudaStream_t st)
+// Initial dt of one member that joins a running batch: phase 0 over its own
+// units (a work list of its tiles), the other members untouched.
+int Batch::initial_dt_of(DevScenario *s)
+{
+    int slot = -1;
+    for (int i = 0; i < capacity; i++)
+        if (members[i] == s) slot = i;
+    if (slot < 0) return THY_ERR_INVALID;
+    std::vector<int2> w(s->desc.ntiles);
+    for (int t = 0; t < s->desc.ntiles; t++) w[t] = make_int2(slot, t);
+    const int n = (int)w.size();
+    if (n > work_capacity) return THY_ERR_INVALID;
+    int rc;
+    if ((rc = s->upload_ctl(st))) return rc;
+    THY_CK(cudaMemcpyAsync(d_work0, w.data(), n * sizeof(int2), cudaMemcpyHostToDevice, st));
+    THY_CK(cudaMemcpyAsync(d_nwork0, &n, sizeof(int), cudaMemcpyHostToDevice, st));
+    StepLaunch L = params();
+    L.work = d_work0;
+    L.nwork = d_nwork0;
+    launch_initial_dt(L, st);
+    THY_CK(cudaGetLastError());
+    THY_CK(cudaMemcpyAsync(&h_ctl[slot], d_ctl + slot, sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, st));
+    THY_CK(cudaStreamSynchronize(st));
+    s->hctl = h_ctl[slot];
+    truncate_initial_dt(s);
+    return THY_OK;
+}
+
+// Host side of one loop iteration's events (src/GPU/ShallowWater.cu:398-421);
+// *changed: a fault deformed the state.
+int handle_events_ex(DevScenario &s, const thy_outputs *o, cudaStream_t st, bool *changed)
 {
     int rc;
+    const int f0 = s.hctl.fault_next;
     if ((rc = s.apply_due_faults(st))) return rc;
+    if (changed) *changed = s.hctl.fault_next != f0;
     if (s.save_nc >= 0.0 && s.hctl.t >= s.hctl.next_nc) {
         s.hctl.next_nc += s.save_nc;
         if ((rc = s.snapshot(o, st))) return rc;
@@ -751,8 +820,11 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
             if (!(s.hctl.t < s.t_end)) break;
             if (s.max_steps >= 0 && s.hctl.step >= s.max_steps) break;
             if (s.hctl.status == kFailed) { rc = THY_ERR_NONFINITE; goto out; }
-            if ((rc = handle_events(s, o, st))) goto out;
-            if ((rc = b.reset_lists())) goto out;
+            {
+                bool changed = false;
+                if ((rc = handle_events_ex(s, o, st, &changed))) goto out;
+                if (changed && (rc = b.reset_lists())) goto out;
+            }
             s.hctl.status = kRunning;
             s.hctl.events = 0;
             if ((rc = s.upload_ctl(st))) goto out;

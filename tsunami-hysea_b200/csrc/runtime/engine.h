@@ -89,6 +89,8 @@ struct Batch {
     ScenarioDev *d_table = nullptr;
     int2 *d_work = nullptr;
     int *d_nwork = nullptr;
+    int2 *d_work0 = nullptr;           // work list of scenarios joining (their initial dt)
+    int *d_nwork0 = nullptr;
     int *d_lists = nullptr;            // deep / general lists of the current step (StepLaunch::lists)
     ScenarioCtl *d_ctl = nullptr;      // slots
     ScenarioCtl *h_ctl = nullptr;      // pinned mirror
@@ -110,7 +112,10 @@ struct Batch {
     int init(int capacity, int max_work, cudaStream_t stream);
     int attach(DevScenario *s);      // gives s a control slot
     int detach(DevScenario *s);
-    int rebuild();                    // tables + work list of RUNNING members; recapture the graph
+    int update();                     // upload the member table and the work list, reset the lists
+    int capture();                    // (re)capture the step graph for the current capacity
+    int rebuild();                    // update(), and capture() when there is no graph yet
+    int initial_dt_of(DevScenario *s);   // initial dt of one member (phase 0 over its units only)
     int run_chunk(bool timed);       // one graph launch + control download (synchronous)
     StepLaunch params() const;
     int reset_lists();               // all items general: after the host changed a member's state

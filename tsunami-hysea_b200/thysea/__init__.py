@@ -19,6 +19,8 @@ import numpy as np
 from . import _ffi, synth  # noqa: F401
 
 THY_OK = 0
+THY_ERR_GPU_MEMORY, THY_ERR_HOST, THY_ERR_INVALID, THY_ERR_CUDA, THY_ERR_NO_DEVICE = 1, 2, 3, 4, 5
+THY_ERR_NONFINITE, THY_ERR_BUDGET, THY_ERR_CANCELLED, THY_ERR_TOO_LARGE = 6, 7, 8, 9
 
 
 class ThyError(RuntimeError):
@@ -262,6 +264,75 @@ class Session:
     def close(self):
         if getattr(self, "_h", None):
             _ffi.lib().thy_session_close(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """Multi-scenario runtime (thy_server_*): requests are admitted under an
+    HBM budget and stepped together in one batch; results arrive through
+    completion callbacks, collected in `results` (request id -> dict with
+    status, stats and the output fields)."""
+
+    def __init__(self, hbm_budget_bytes: int = 0, max_scenarios: int = 0, device: int = 0):
+        L = _ffi.lib()
+        o = _ffi.ServerOpts(int(hbm_budget_bytes), int(max_scenarios), int(device))
+        h = ctypes.c_void_p()
+        _check(L.thy_server_open(ctypes.byref(o), ctypes.byref(h)), "thy_server_open")
+        self._h = h
+        self._live = {}
+        self.results: Dict[int, Dict] = {}
+        self._cb = _ffi.DoneFn(self._done)
+
+    def _done(self, user, request, status, stats_ptr):
+        keep = self._live.pop(int(request), None)
+        res = {"status": int(status), "outputs": keep["fields"] if keep else None, "stats": None}
+        if stats_ptr:
+            st = ctypes.cast(stats_ptr, ctypes.POINTER(_ffi.Stats)).contents
+            res["stats"] = {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+        if keep:
+            res["problem"] = keep["prep"]
+        self.results[int(request)] = res
+
+    def submit(self, problem, out: Optional[Dict[str, np.ndarray]] = None) -> int:
+        """Queues a scenario (a synth.Problem or a Prepared); returns the request id."""
+        prep = problem if isinstance(problem, Prepared) else Prepared(problem)
+        ny, nx = int(prep.c.ny), int(prep.c.nx)
+        fields = out if out is not None else {k: np.empty((ny, nx), np.float32) for k in OUTPUT_FIELDS}
+        o = _ffi.Outputs()
+        for k in OUTPUT_FIELDS:
+            setattr(o, k, _p(fields[k], _ffi.f32p))
+        rid = ctypes.c_longlong()
+        _check(_ffi.lib().thy_server_submit(self._h, prep.view, ctypes.byref(o), self._cb, None, ctypes.byref(rid)),
+               "thy_server_submit")
+        self._live[rid.value] = {"prep": prep, "fields": fields, "outputs": o}
+        return rid.value
+
+    def cancel(self, request: int):
+        _check(_ffi.lib().thy_server_cancel(self._h, int(request)), "thy_server_cancel")
+
+    def progress(self) -> int:
+        """One round (admit, events, one chunk of steps, retire); returns queued + running."""
+        active = ctypes.c_int()
+        _check(_ffi.lib().thy_server_progress(self._h, ctypes.byref(active)), "thy_server_progress")
+        return active.value
+
+    def drain(self):
+        _check(_ffi.lib().thy_server_drain(self._h), "thy_server_drain")
+
+    def stats(self) -> Dict:
+        st = _ffi.ServerStats()
+        _check(_ffi.lib().thy_server_get_stats(self._h, ctypes.byref(st)), "thy_server_get_stats")
+        return {k: getattr(st, k) for k, _ in _ffi.ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _ffi.lib().thy_server_close(self._h)
             self._h = None
 
     def __del__(self):

@@ -72,6 +72,22 @@ class Stats(ctypes.Structure):
     ]
 
 
+class ServerOpts(ctypes.Structure):
+    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("max_scenarios", ctypes.c_int), ("device", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [
+        ("submitted", ctypes.c_longlong), ("admitted", ctypes.c_longlong), ("completed", ctypes.c_longlong),
+        ("failed", ctypes.c_longlong), ("cancelled", ctypes.c_longlong), ("rejected", ctypes.c_longlong),
+        ("chunks", ctypes.c_longlong), ("queued", ctypes.c_int), ("running", ctypes.c_int),
+        ("hbm_in_use", ctypes.c_longlong), ("hbm_budget", ctypes.c_longlong),
+        ("device_ms", ctypes.c_double), ("cell_updates", ctypes.c_double),
+    ]
+
+
+DoneFn = ctypes.CFUNCTYPE(None, ctypes.c_void_p, ctypes.c_longlong, ctypes.c_int, ctypes.c_void_p)
+
 # names and signatures of every function include/thysea.h declares
 SIGNATURES = {
     "thy_version": ([], ctypes.c_char_p),
@@ -109,6 +125,14 @@ SIGNATURES = {
     "thy_session_tiles": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                            ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "thy_session_close": ([ctypes.c_void_p], None),
+    "thy_server_open": ([ctypes.POINTER(ServerOpts), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
+    "thy_server_submit": ([ctypes.c_void_p, ctypes.POINTER(ProblemC), ctypes.POINTER(Outputs), DoneFn,
+                           ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "thy_server_cancel": ([ctypes.c_void_p, ctypes.c_longlong], ctypes.c_int),
+    "thy_server_progress": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)], ctypes.c_int),
+    "thy_server_drain": ([ctypes.c_void_p], ctypes.c_int),
+    "thy_server_get_stats": ([ctypes.c_void_p, ctypes.POINTER(ServerStats)], ctypes.c_int),
+    "thy_server_close": ([ctypes.c_void_p], None),
 }
 
 _lib = None
