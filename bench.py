@@ -345,6 +345,177 @@ def run_reference(a, dist: Dist):
     }
 
 
+def _pct(xs, q):
+    import numpy as np
+
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
+
+
+def _plain_service(preps, out_fields):
+    """One-at-a-time path: thy_run per scenario (an iterable of Prepared,
+    made lazily by the caller if it likes), back to back; returns the service
+    time of each (s) and the cell updates."""
+    import thysea
+
+    times, cu = [], 0.0
+    for prep in preps:
+        t0 = time.perf_counter()
+        r = thysea.run(prep, snapshots=False, series=False, out=out_fields(prep))
+        times.append(time.perf_counter() - t0)
+        cu += float(prep.c.nx) * float(prep.c.ny) * float(r["iterations"])
+    return times, cu
+
+
+def _fifo(arrivals, service):
+    """Time-to-result of a single FIFO server with the given arrivals and
+    service times (the plain path serving the same stream)."""
+    free, ttr, last = 0.0, [], 0.0
+    for t_a, t_s in zip(arrivals, service):
+        start = max(t_a, free)
+        free = start + t_s
+        ttr.append(free - t_a)
+        last = free
+    return ttr, last
+
+
+def run_batched(a, dist):
+    """BASELINE configs 3-5 through the multi-scenario runtime (thy_server),
+    next to the plain path (one thy_run per scenario) on the same inputs.
+
+      batch:   64 scenarios on one shared 2048^2 bathymetry, one seeded
+               Okada fault each, 1800 s, all submitted at once;
+      mixed:   32 scenarios, sides log-uniform 256-4096, own bathymetry and
+               fault, 600-7200 s, all submitted at once;
+      serving: Poisson arrivals (--rate req/s for --duration s) of config-4
+               requests under a 150 GB HBM budget; problems are prepared by
+               a background thread ahead of their arrival; time-to-result =
+               arrival -> outputs on the host.  Grid sides are drawn
+               log-uniformly and rounded to a multiple of 64 so that one
+               seeded bathymetry per side serves all its requests (each
+               request keeps its own seeded fault and duration).
+    """
+    import concurrent.futures as cf
+    import math
+
+    import numpy as np
+
+    import thysea
+    from thysea import synth
+
+    thysea._ffi.lib().thy_set_device(dist.local)
+    pinned_cache = {}
+
+    def out_fields(prep):
+        key = (int(prep.c.ny), int(prep.c.nx))
+        if key not in pinned_cache:
+            pinned_cache[key] = thysea.PinnedOutputs(prep)
+        return pinned_cache[key].fields
+
+    budget = int(a.budget_gb * 1e9)
+    if a.workload in ("batch", "mixed"):
+        probs = synth.batch_uniform(count=a.count or 64) if a.workload == "batch" else synth.mixed(count=a.count or 32)
+        preps = [thysea.Prepared(p).pin() for p in probs]
+        cells = [float(p.nx) * float(p.ny) for p in probs]
+        # batched: everything submitted at t = 0
+        srv = thysea.Server(hbm_budget_bytes=budget)
+        dist.barrier()
+        t0 = time.perf_counter()
+        ids = [srv.submit(pr, out=out_fields(pr)) for pr in preps]
+        srv.drain()
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        res = [srv.results[i] for i in ids]
+        srv.close()
+        ok = all(r["status"] == 0 for r in res)
+        ttr = [r["done_at"] - t0 for r in res]
+        cu = sum(c * r["stats"]["steps"] for c, r in zip(cells, res))
+        # plain: one thy_run per scenario
+        p_times, p_cu = _plain_service(preps, out_fields)
+        p_wall = sum(p_times)
+        p_ttr = list(np.cumsum(p_times))
+        line = {
+            "metric": "scenarios/hour", "value": round(len(probs) / wall * 3600.0, 1), "unit": "scenarios/h",
+            "n_gpus": dist.world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)",
+            "config": {"workload": a.workload, "scenarios": len(probs),
+                       "cells_total": int(sum(cells)), "hbm_budget_gb": a.budget_gb},
+            "all_ok": ok, "wall_s": round(wall, 3), "cell_updates_per_s": round(cu / wall, 1),
+            "device_s": round(st["device_ms"] / 1e3, 3), "chunks": st["chunks"],
+            "time_to_result_p50_s": round(_pct(ttr, 50), 3), "time_to_result_p99_s": round(_pct(ttr, 99), 3),
+            "plain": {"scenarios_per_hour": round(len(probs) / p_wall * 3600.0, 1), "wall_s": round(p_wall, 3),
+                      "cell_updates_per_s": round(p_cu / p_wall, 1),
+                      "time_to_result_p50_s": round(_pct(p_ttr, 50), 3),
+                      "time_to_result_p99_s": round(_pct(p_ttr, 99), 3)},
+        }
+        return line
+
+    # ---- serving ----
+    rng = np.random.default_rng(5)
+    arrivals = synth.poisson_arrivals(rate=a.rate, duration=a.duration, seed=5)
+    sides = [int(64 * round(math.exp(rng.uniform(math.log(256), math.log(4096))) / 64)) for _ in arrivals]
+    seeds = rng.integers(1 << 30, size=len(arrivals))
+    t_sim = rng.uniform(600.0, 7200.0, size=len(arrivals))
+    bathy = {}
+
+    def make(k):
+        n = sides[k]
+        if n not in bathy:
+            r0 = np.random.default_rng(1000 + n)
+            lon, lat = synth.lonlat_grid(n, n)
+            bathy[n] = (lon, lat, synth.shelf_bathymetry(n, n, r0))
+        lon, lat, z = bathy[n]
+        rr = np.random.default_rng(int(seeds[k]))
+        p = synth.Problem(name=f"req{k:04d}", lon=lon, lat=lat, z=z, faults=[synth.random_fault(lon, lat, z, rr)],
+                          sim_time=float(t_sim[k]))
+        return thysea.Prepared(p)
+
+    lead = 4.0   # seconds of look-ahead for the preparing thread
+    pool = cf.ThreadPoolExecutor(max_workers=2)
+    futs = {}
+    srv = thysea.Server(hbm_budget_bytes=budget)
+    t0 = time.perf_counter()
+    nxt, submitted, rid_to_k = 0, 0, {}
+    while True:
+        now = time.perf_counter() - t0
+        while nxt < len(arrivals) and arrivals[nxt] <= now + lead:
+            futs[nxt] = pool.submit(make, nxt)
+            nxt += 1
+        while submitted < len(arrivals) and arrivals[submitted] <= now:
+            prep = futs.pop(submitted).result()
+            rid_to_k[srv.submit(prep, out=out_fields(prep))] = submitted
+            submitted += 1
+        active = srv.progress()
+        if submitted == len(arrivals) and active == 0:
+            break
+        if active == 0:
+            time.sleep(max(0.0, min(0.005, arrivals[submitted] - (time.perf_counter() - t0))))
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    res = {k: srv.results[r] for r, k in rid_to_k.items()}
+    srv.close()
+    ok = all(r["status"] == 0 for r in res.values())
+    ttr = [res[k]["done_at"] - t0 - arrivals[k] for k in sorted(res)]
+    cu = sum(float(sides[k]) ** 2 * res[k]["stats"]["steps"] for k in res)
+    # plain path: measured service times of the same requests, FIFO over the same arrivals
+    p_times, p_cu = _plain_service((make(k) for k in range(len(arrivals))), out_fields)
+    p_ttr, p_end = _fifo(list(arrivals), p_times)
+    return {
+        "metric": "scenarios/hour", "value": round(len(res) / wall * 3600.0, 1), "unit": "scenarios/h",
+        "n_gpus": dist.world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded)",
+        "config": {"workload": "serving", "rate_per_s": a.rate, "duration_s": a.duration, "requests": len(arrivals),
+                   "hbm_budget_gb": a.budget_gb, "sides": "log-uniform 256-4096 (multiples of 64)",
+                   "sim_time_s": "uniform 600-7200"},
+        "all_ok": ok, "wall_s": round(wall, 3), "cell_updates": cu, "cell_updates_per_s": round(cu / wall, 1),
+        "device_busy_s": round(st["device_ms"] / 1e3, 3),
+        "time_to_result_p50_s": round(_pct(ttr, 50), 3), "time_to_result_p99_s": round(_pct(ttr, 99), 3),
+        "plain": {"scenarios_per_hour": round(len(arrivals) / p_end * 3600.0, 1),
+                  "time_to_result_p50_s": round(_pct(p_ttr, 50), 3),
+                  "time_to_result_p99_s": round(_pct(p_ttr, 99), 3),
+                  "service_s_total": round(sum(p_times), 3), "cell_updates_per_s": round(p_cu / sum(p_times), 1)},
+    }
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -357,11 +528,22 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=400)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
+    ap.add_argument("--workload", choices=["single", "batch", "mixed", "serving"], default="single",
+                    help="single: config 2 (the headline line); batch / mixed / serving: configs 3 / 4 / 5")
+    ap.add_argument("--count", type=int, default=0, help="batch / mixed: number of scenarios (0: 64 / 32)")
+    ap.add_argument("--rate", type=float, default=2.0, help="serving: requests per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
+    ap.add_argument("--budget-gb", type=float, default=150.0, help="batch / mixed / serving: HBM budget")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     dist = Dist()
     try:
-        line = run_reference(a, dist) if a.impl == "reference" else run_ours(a, dist)
+        if a.impl == "reference":
+            line = run_reference(a, dist)
+        elif a.workload != "single":
+            line = run_batched(a, dist)
+        else:
+            line = run_ours(a, dist)
         if line is not None and dist.rank == 0:
             print(json.dumps(line), flush=True)
     finally:

@@ -12,6 +12,7 @@ would drive its shallowWater() through a small FFI stub.
 from __future__ import annotations
 
 import ctypes
+import time
 from typing import Dict, Optional
 
 import numpy as np
@@ -291,12 +292,11 @@ class Server:
 
     def _done(self, user, request, status, stats_ptr):
         keep = self._live.pop(int(request), None)
-        res = {"status": int(status), "outputs": keep["fields"] if keep else None, "stats": None}
+        res = {"status": int(status), "outputs": keep["fields"] if keep else None, "stats": None,
+               "done_at": time.perf_counter()}
         if stats_ptr:
             st = ctypes.cast(stats_ptr, ctypes.POINTER(_ffi.Stats)).contents
             res["stats"] = {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
-        if keep:
-            res["problem"] = keep["prep"]
         self.results[int(request)] = res
 
     def submit(self, problem, out: Optional[Dict[str, np.ndarray]] = None) -> int:
