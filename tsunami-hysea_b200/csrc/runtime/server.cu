@@ -38,6 +38,7 @@ struct Active {
     std::unique_ptr<DevScenario> s;
     bool fresh = true;            // admitted, its first events not handled yet
     bool cancelled = false;
+    bool deferred = false;        // resident but not stepped in the coming chunk
     Clock::time_point admitted;
 };
 
@@ -48,6 +49,7 @@ struct thy_server {
     cudaStream_t st = nullptr;
     thy::Batch b;
     size_t budget = 0, in_use = 0;
+    long long chunk_cells = 0;    // < 0: step every resident scenario
     long long next_id = 1;
     std::deque<thy::Request> queue;
     std::vector<thy::Active *> slots;     // by batch slot
@@ -143,6 +145,7 @@ extern "C" int thy_server_open(const thy_server_opts *opts, thy_server **out)
     THY_CK(cudaMemGetInfo(&free_b, &total_b));
     thy_server *S = new thy_server();
     S->budget = o.hbm_budget_bytes ? (size_t)o.hbm_budget_bytes : free_b / 10 * 9;
+    S->chunk_cells = o.chunk_cells ? o.chunk_cells : 32ll << 20;
     const int cap = o.max_scenarios > 0 ? o.max_scenarios : 256;
     // work-list capacity: the tiles of the budget's worth of cells, at least one grid of 4096^2
     const size_t cells = S->budget / 40 + (size_t)4096 * 4096;
@@ -201,8 +204,9 @@ extern "C" int thy_server_cancel(thy_server *S, long long request)
     return THY_ERR_INVALID;
 }
 
-// One round: admit, perform due events, run one chunk of steps for every
-// running scenario, retire the finished, cancelled and failed ones.
+// One round: admit, perform due events, run one chunk of steps for the
+// scenarios the chunk's work budget selects, retire the finished, cancelled
+// and failed ones.
 extern "C" int thy_server_progress(thy_server *S, int *active)
 {
     if (!S) return THY_ERR_INVALID;
@@ -227,7 +231,7 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             complete(S, i, THY_OK);
             continue;
         }
-        if (a->fresh || s.hctl.status != kRunning) {
+        if (a->fresh || (s.hctl.status != kRunning && !a->deferred)) {
             bool changed = false;
             if ((rc = handle_events_ex(s, a->r.o, S->st, &changed))) {
                 complete(S, i, rc);
@@ -237,9 +241,40 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             a->fresh = false;
             s.hctl.status = kRunning;
             s.hctl.events = 0;
+            a->deferred = false;
             if ((rc = s.upload_ctl(S->st))) return rc;
         }
         any_running = true;
+    }
+    // Work budget of the chunk: the resident scenarios with the least
+    // remaining work (cells x remaining steps at the current dt) are stepped
+    // until their cells reach chunk_cells; the others wait (status idle on
+    // the device, so every kernel skips them).  Small requests are batched,
+    // a large one runs nearly alone, and no request's arithmetic changes.
+    if (any_running) {
+        std::vector<std::pair<double, int>> order;
+        for (int i = 0; i < cap; i++) {
+            Active *a = S->slots[i];
+            if (!a) continue;
+            const DevScenario &s = *a->s;
+            const double cells = (double)s.nx * s.ny;
+            const double steps = s.hctl.dt > 0.0 ? (s.t_end - s.hctl.t) / s.hctl.dt : 0.0;
+            order.emplace_back(cells * std::max(steps, 1.0), i);
+        }
+        std::sort(order.begin(), order.end());
+        double taken = 0.0;
+        for (const auto &e : order) {
+            Active *a = S->slots[e.second];
+            DevScenario &s = *a->s;
+            const bool step = S->chunk_cells < 0 || taken < (double)S->chunk_cells;
+            if (step) taken += (double)s.nx * s.ny;
+            const int want = step ? kRunning : kIdle;
+            if (s.hctl.status != want || a->deferred == step) {
+                s.hctl.status = want;
+                a->deferred = !step;
+                if ((rc = s.upload_ctl(S->st))) return rc;
+            }
+        }
     }
     if (S->members_changed) {
         if ((rc = S->b.rebuild())) return rc;   // table + work list (+ lists reset)

@@ -280,9 +280,9 @@ class Server:
     completion callbacks, collected in `results` (request id -> dict with
     status, stats and the output fields)."""
 
-    def __init__(self, hbm_budget_bytes: int = 0, max_scenarios: int = 0, device: int = 0):
+    def __init__(self, hbm_budget_bytes: int = 0, max_scenarios: int = 0, device: int = 0, chunk_cells: int = 0):
         L = _ffi.lib()
-        o = _ffi.ServerOpts(int(hbm_budget_bytes), int(max_scenarios), int(device))
+        o = _ffi.ServerOpts(int(hbm_budget_bytes), int(max_scenarios), int(device), int(chunk_cells))
         h = ctypes.c_void_p()
         _check(L.thy_server_open(ctypes.byref(o), ctypes.byref(h)), "thy_server_open")
         self._h = h

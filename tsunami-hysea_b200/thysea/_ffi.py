@@ -73,7 +73,8 @@ class Stats(ctypes.Structure):
 
 
 class ServerOpts(ctypes.Structure):
-    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("max_scenarios", ctypes.c_int), ("device", ctypes.c_int)]
+    _fields_ = [("hbm_budget_bytes", ctypes.c_longlong), ("max_scenarios", ctypes.c_int), ("device", ctypes.c_int),
+                ("chunk_cells", ctypes.c_longlong)]
 
 
 class ServerStats(ctypes.Structure):
