@@ -19,9 +19,10 @@
 // writes, so every tile is stepped by exactly one of them.
 // Phase 0 (the general template) computes the initial dt.
 //
-// Row marching: a tile is kWarps column strips side by side; in a strip each
-// lane owns one column and the warp marches down the tile's rows keeping a
-// five-row window of its column in registers.  The y edge below the current
+// Row marching (general kernel): a unit is 4 column strips side by side, each
+// in two row groups of 8 rows, one warp per strip and group; each lane owns
+// one column and the warp marches down its rows keeping a five-row window of
+// its column in registers.  The y edge below the current
 // row needs nothing but that window; x edges take their left/right
 // neighbours from warp shuffles.  The 32 lanes cover 28 output columns plus
 // a two-column halo on each side (the x stencil reaches two cells), so the
@@ -42,11 +43,13 @@
 
 namespace thy {
 
-constexpr int NT = kStepThreads;
-constexpr int WARPS = NT / 32;
-constexpr int OUTW = 28;              // output columns per warp
+constexpr int STRIPS = kStepThreads / 32;   // column strips of a tile
+constexpr int OUTW = 28;              // output columns per strip
 constexpr int TY = kTileY;            // output rows per tile
-static_assert(kTileX == WARPS * OUTW, "tile width = warps x 28 columns");
+static_assert(kTileX == STRIPS * OUTW, "tile width = strips x 28 columns");
+constexpr int GWARPS = 2 * STRIPS;    // general kernel: every strip of a unit in two row groups
+constexpr int GNT = 32 * GWARPS;
+constexpr int GROWS = kHalfRows / 2;  // rows a general-kernel warp marches
 
 // one cell of a lane's column: depth, surface elevation, still-water depth, discharges
 struct Cell {
@@ -829,17 +832,18 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
     }
 }
 
-// General kernel, one work unit (half tile) per CTA iteration: phase 0 over
-// every unit of the work list, phases 1 and 2 over the general list of the
-// step.
+// General kernel, one work unit (half tile) per CTA iteration, 8 warps (4
+// column strips x 2 row groups): phase 0 over every unit of the work list,
+// phases 1 and 2 over the general list of the step.
 template <int PHASE>
-__global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                                  const int *__restrict__ nwork_ptr, const int *__restrict__ lists,
-                                                  int cap)
+__global__ void __launch_bounds__(GNT) step_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+                                                   const int *__restrict__ nwork_ptr, const int *__restrict__ lists,
+                                                   int cap)
 {
-    __shared__ float red[WARPS];          // phases 0 / 2: dt per warp
-    __shared__ float2 slots[9 * WARPS];   // phase 1: unit summary per warp
+    __shared__ float red[GWARPS];          // phases 0 / 2: dt per warp
+    __shared__ float2 slots[9 * GWARPS];   // phase 1: unit summary per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int strip = warp % STRIPS, group = warp / STRIPS;
     const int nitems = (PHASE == 0) ? 2 * *nwork_ptr : lists[1];
     for (int g = blockIdx.x; g < nitems; g += gridDim.x) {
         const int u = (PHASE == 0) ? g : general_items(lists, cap)[g];
@@ -851,8 +855,11 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         const int nx = s.nx, ny = s.ny;
         const int ty = item.y / s.tiles_x, tx = item.y - ty * s.tiles_x;
         const int uy = 2 * ty + (u & 1);
-        const int x0 = tx * kTileX + warp * OUTW, y0 = uy * kHalfRows;
-        if (y0 >= ny) continue;   // a unit below the grid (phase 0 only; never listed)
+        const int uy0 = uy * kHalfRows;
+        if (uy0 >= ny) continue;   // a unit below the grid (phase 0 only; never listed)
+        const int unit_end = min(uy0 + kHalfRows, ny);
+        // this warp: column strip `strip`, rows y0 .. y_end-1 of the unit
+        const int x0 = tx * kTileX + strip * OUTW, y0 = uy0 + group * GROWS;
         const int p = ctl->parity;
         const float dt = (float)ctl->dt;
         const float t_sec = (float)(ctl->t * ctl->T);
@@ -860,7 +867,7 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         const int col = map_col(gx, nx, s.periodic);
         const bool has_edge = (lane >= 2) && (lane <= 30) && (gx <= nx);
         const bool has_cell = (lane >= 2) && (lane <= 29) && (gx < nx);
-        const int y_end = min(y0 + kHalfRows, ny);
+        const int y_end = min(y0 + GROWS, unit_end);
         const float *eta_in = (PHASE == 2) ? s.eta[p ^ 1] : s.eta[p];
         const float *qx_in = s.qx[p], *qy_in = s.qy[p];
         const size_t pitch = (size_t)s.pitch;
@@ -872,7 +879,7 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
         hacc.init();
         bool bad = false;
 
-        if (x0 < nx) {
+        if (x0 < nx && y0 < y_end) {
             constexpr bool DIAG = (PHASE == 1);
             Cell c0 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 2, ny) * pitch + col);
             Cell c1 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 1, ny) * pitch + col);
@@ -1005,7 +1012,7 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
                         }
                         if (!isfinite(eta)) bad = true;
                         s.eta[p ^ 1][idx] = eta;
-                        hacc.add(eta + D, yo - y0 < 2, y_end - yo <= 2);
+                        hacc.add(eta + D, yo - uy0 < 2, unit_end - yo <= 2);
                     } else {
                         // momentum update (src/GPU/Volumen_kernel.cu:175-219)
                         const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
@@ -1087,10 +1094,10 @@ __global__ void __launch_bounds__(NT) step_kernel(const ScenarioDev *__restrict_
             if (lane == 0) red[warp] = local_min;
         }
         __syncthreads();
-        if (PHASE == 1) store_unit_summary(&s.usum[p ^ 1][(size_t)uy * s.tiles_x + tx], slots, WARPS);
+        if (PHASE == 1) store_unit_summary(&s.usum[p ^ 1][(size_t)uy * s.tiles_x + tx], slots, GWARPS);
         if (PHASE != 1 && threadIdx.x == 0) {
             float m = red[0];
-            for (int k = 1; k < WARPS; k++) m = fminf(m, red[k]);
+            for (int k = 1; k < GWARPS; k++) m = fminf(m, red[k]);
             atomicMin(&ctl->dt_bits, __float_as_uint(m));
             if (PHASE == 0) {
                 // initial dt: the last tile stores the min and resets the counters
@@ -1125,7 +1132,7 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
     case 0:
         deep_kernel<1><<<L.deep_grid[0], DNT, deep_smem_bytes(1), st>>>(L.scen, L.work, L.lists);
         break;
-    case 1: step_kernel<1><<<L.grid, NT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    case 1: step_kernel<1><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
     case 2:
         cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
         classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0);
@@ -1133,14 +1140,14 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
     case 3:
         deep_kernel<2><<<L.deep_grid[1], DNT, deep_smem_bytes(2), st>>>(L.scen, L.work, L.lists);
         break;
-    case 4: step_kernel<2><<<L.grid, NT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    case 4: step_kernel<2><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
     default: controller_kernel<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.scen, L.nslots); break;
     }
 }
 
 void launch_initial_dt(const StepLaunch &L, cudaStream_t st)
 {
-    step_kernel<0><<<L.grid, NT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap);
+    step_kernel<0><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap);
 }
 
 void launch_lists_all_general(const StepLaunch &L, cudaStream_t st)
@@ -1163,7 +1170,7 @@ cudaError_t configure_step_kernels()
 int step_blocks_per_sm()
 {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2>, NT, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2>, GNT, 0);
     return n;
 }
 
