@@ -451,9 +451,12 @@ __device__ __forceinline__ void tmap_acquire(const TmaMap *map)
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
 }
 
-constexpr int DWARPS = 8;                           // 4 column strips x 2 row groups
-constexpr int DNT = DWARPS * 32;
-constexpr int DROWS = kHalfRows / 2;                // rows a warp marches
+// Warps of a deep-kernel CTA: 4 column strips x row groups.  Phase 1 (two
+// CTAs per SM: its double-buffered staging is larger) uses 3 row groups so
+// that 24 warps per SM hide the latency; phase 2 uses 2 at three CTAs per SM.
+__host__ __device__ constexpr int deep_groups(int phase) { return phase == 1 ? 3 : 2; }
+__host__ __device__ constexpr int deep_warps(int phase) { return 4 * deep_groups(phase); }
+__host__ __device__ constexpr int deep_threads(int phase) { return 32 * deep_warps(phase); }
 constexpr int SPLANE = (kStageRows * kStageW + 31) / 32 * 32;   // floats per staged plane (128-byte multiple)
 constexpr int DPLANE = kHalfRows * kTileX;          // floats per staged diagnostics plane
 constexpr uint32_t kStateBytes = kStageRows * kStageW * 4;
@@ -477,7 +480,7 @@ struct DeepRow {
 __host__ __device__ constexpr size_t deep_misc_offset(int phase) { return 2 * deep_stage_bytes(phase); }
 static size_t deep_smem_bytes(int phase)
 {
-    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + 2 * DWARPS * sizeof(float);
+    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + 2 * deep_warps(phase) * sizeof(float);
 }
 
 // one cell of a staged row (shared memory; the depth is formed here)
@@ -632,10 +635,10 @@ __device__ __forceinline__ void deep_issue(const DeepUnit &d, float *stage, uint
 // window - its rows plus one above and one below, columns x0-4 .. x0+115 of
 // eta, dep, qx, qy, and in phase 1 the diagnostics of its own cells - is
 // staged by TMA, the next unit's copy in flight while the current one is
-// computed.  Warp w marches rows 8 (w >> 2) .. +7 of column strip w & 3 (28
+// computed.  Warp w marches its row group (w >> 2) of column strip w & 3 (28
 // output columns, lanes 2..29) with a two-row window.
 template <int PHASE>
-__global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+__global__ void __launch_bounds__(deep_threads(PHASE), PHASE == 1 ? 2 : 3) deep_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                                    const int *__restrict__ lists)
 {
     extern __shared__ __align__(1024) unsigned char dsm[];
@@ -645,7 +648,10 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
     DeepRow *rows = reinterpret_cast<DeepRow *>(dsm + deep_misc_offset(PHASE) + 16);
     float *red = reinterpret_cast<float *>(rows + kStageRows);   // per warp: dt, or depth min and max
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    constexpr int NW = deep_warps(PHASE), NG = deep_groups(PHASE);
     const int strip = warp & 3, group = warp >> 2;
+    // this warp's rows of the unit: kHalfRows * group / NG .. kHalfRows * (group + 1) / NG - 1
+    const int row0 = kHalfRows * group / NG, nrows = kHalfRows * (group + 1) / NG - row0;
     const int nunits = lists[0];
     if (blockIdx.x >= nunits) return;
     // TMA destinations must be 128-byte aligned: a misaligned buffer is
@@ -701,7 +707,7 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
             const float dt = (float)ctl->dt;
             const float t_sec = (float)(ctl->t * ctl->T);
             const int pitch = s.pitch;
-            const int r_first = group * DROWS + 1;                  // staged row of this warp's first output row
+            const int r_first = row0 + 1;                           // staged row of this warp's first output row
             const int sc = strip * 28 + 2 + lane;                   // staged column of this lane
             const int gx = x0 - 4 + sc;                             // grid column
             const bool has_cell = (lane >= 2) && (lane <= 29);
@@ -731,7 +737,7 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
             float *out0 = (PHASE == 1) ? s.eta[p ^ 1] : s.qx[p ^ 1];
             float *out1 = s.qy[p ^ 1];
             int off = (yb + r_first - 1) * pitch + gx;
-            for (int k = 0; k < DROWS; k++, i += kStageW, off += pitch) {
+            for (int k = 0; k < nrows; k++, i += kStageW, off += pitch) {
                 const DeepRow rn = rows[r_first + k + 1];
                 const Cell n = staged_cell(stage, i + kStageW);
                 const float area = rc.m.z;
@@ -807,19 +813,19 @@ __global__ void __launch_bounds__(DNT, 3) deep_kernel(const ScenarioDev *__restr
             }
             if (lane == 0) {
                 red[warp] = local_min;
-                if (PHASE == 1) red[DWARPS + warp] = local_max;
+                if (PHASE == 1) red[NW + warp] = local_max;
             }
         }
         __syncthreads();   // every warp is done with the staged window and the row metrics
         if (d.run && threadIdx.x == 0) {
             float m = red[0];
-            for (int k = 1; k < DWARPS; k++) m = fminf(m, red[k]);
+            for (int k = 1; k < NW; k++) m = fminf(m, red[k]);
             if (PHASE == 1) {
                 // a deep unit reports its whole-unit {min, max} for its strips
                 // and corners too: conservative for a neighbour's deep test,
                 // and a wet unit fails a neighbour's dry test either way
-                float mx = red[DWARPS];
-                for (int k = 1; k < DWARPS; k++) mx = fmaxf(mx, red[DWARPS + k]);
+                float mx = red[NW];
+                for (int k = 1; k < NW; k++) mx = fmaxf(mx, red[NW + k]);
                 const float2 v = make_float2(m, mx);
                 s.usum[p ^ 1][d.uidx] = UnitSum{v, v, v, v, v, v, v, v, v};
             } else {
@@ -1130,7 +1136,7 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
 {
     switch (k) {
     case 0:
-        deep_kernel<1><<<L.deep_grid[0], DNT, deep_smem_bytes(1), st>>>(L.scen, L.work, L.lists);
+        deep_kernel<1><<<L.deep_grid[0], deep_threads(1), deep_smem_bytes(1), st>>>(L.scen, L.work, L.lists);
         break;
     case 1: step_kernel<1><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
     case 2:
@@ -1138,7 +1144,7 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
         classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0);
         break;
     case 3:
-        deep_kernel<2><<<L.deep_grid[1], DNT, deep_smem_bytes(2), st>>>(L.scen, L.work, L.lists);
+        deep_kernel<2><<<L.deep_grid[1], deep_threads(2), deep_smem_bytes(2), st>>>(L.scen, L.work, L.lists);
         break;
     case 4: step_kernel<2><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
     default: controller_kernel<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.scen, L.nslots); break;
@@ -1177,8 +1183,10 @@ int step_blocks_per_sm()
 int deep_blocks_per_sm(int phase)
 {
     int n = 0;
-    if (phase == 1) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<1>, DNT, deep_smem_bytes(1));
-    else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<2>, DNT, deep_smem_bytes(2));
+    if (phase == 1)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<1>, deep_threads(1), deep_smem_bytes(1));
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<2>, deep_threads(2), deep_smem_bytes(2));
     return n;
 }
 
