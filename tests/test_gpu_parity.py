@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 import oracle
-from parity import ETA_TOL_M, MAXH_REL_L2, compare
+from parity import ETA_TOL_M, MAXH_REL_L2, compare, max_abs_eta
 from thysea import synth
 
 pytestmark = pytest.mark.gpu
@@ -139,3 +139,21 @@ def test_deep_tiles_fault_mid_run(gpu):
     g, r, c = _both(gpu, p)
     _assert_parity(c)
     assert g["deep_tiles"] > 0
+
+
+def test_async_snapshots_and_gauges_in_order(gpu):
+    """snapshots every 20 s and gauges every 10 s are delivered by the writer
+    thread while the GPU steps on: all of them, in order, each the state of
+    its own step (against the oracle's snapshots and gauges)"""
+    p = synth.plain_small(nx=256, ny=192, sim_time=400.0, save_time=20.0, series_time=10.0, npoints=8)
+    p.name = "async_out"
+    g, r, c = _both(gpu, p, max_snaps=32, max_series=64)
+    _assert_parity(c)
+    t = np.asarray(g["snapshots"]["time"])
+    assert len(t) == g["nsnaps"] == r["nsnaps"] and np.all(np.diff(t) > 0)
+    for i in range(len(t)):
+        assert abs(t[i] - r["snapshots"]["time"][i]) < 1e-3
+        assert max_abs_eta(g["snapshots"]["eta"][i], r["snapshots"]["eta"][i]) <= ETA_TOL_M
+    ts = np.asarray(g["series"]["time"])
+    assert len(ts) == g["nseries"] == r["nseries"] and np.all(np.diff(ts) > 0)
+    assert np.abs(np.asarray(g["series"]["eta"]) - r["series"]["eta"]).max() <= ETA_TOL_M

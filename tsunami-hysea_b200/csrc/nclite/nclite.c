@@ -21,6 +21,7 @@
 #include <stdint.h>
 #include <stdio.h>
 #include <stdlib.h>
+#include <pthread.h>
 #include <string.h>
 
 #define NCL_MAX_FILES 64
@@ -70,6 +71,10 @@ typedef struct {
 } ncl_file;
 
 static ncl_file g_files[NCL_MAX_FILES];
+/* guards claiming and freeing slots of g_files: files are opened and closed
+   from several threads (one writer thread per scenario); each open file is
+   used by one thread at a time */
+static pthread_mutex_t g_slots_lock = PTHREAD_MUTEX_INITIALIZER;
 
 /* ------------------------------------------------------------------ */
 /* helpers                                                              */
@@ -261,15 +266,25 @@ static void release(ncl_file *f)
     free_atts(f->gatts, f->ngatts);
     for (i = 0; i < f->nvars; i++) free_atts(f->vars[i].atts, f->vars[i].natts);
     free(f->vars);
+    pthread_mutex_lock(&g_slots_lock);
     memset(f, 0, sizeof(*f));
+    pthread_mutex_unlock(&g_slots_lock);
 }
 
+/* claims a free slot: cleared and marked in use */
 static int alloc_slot(void)
 {
-    int i;
+    int i, id = -1;
+    pthread_mutex_lock(&g_slots_lock);
     for (i = 0; i < NCL_MAX_FILES; i++)
-        if (!g_files[i].in_use) return i;
-    return -1;
+        if (!g_files[i].in_use) {
+            memset(&g_files[i], 0, sizeof(ncl_file));
+            g_files[i].in_use = 1;
+            id = i;
+            break;
+        }
+    pthread_mutex_unlock(&g_slots_lock);
+    return id;
 }
 
 /* ------------------------------------------------------------------ */
@@ -321,8 +336,10 @@ int nc_create(const char *path, int cmode, int *ncidp)
     id = alloc_slot();
     if (id < 0) return NC_ENFILE;
     fp = fopen(path, "w+b");
-    if (!fp) return NC_EIO;
-    memset(&g_files[id], 0, sizeof(ncl_file));
+    if (!fp) {
+        release(&g_files[id]);
+        return NC_EIO;
+    }
     g_files[id].fp = fp;
     g_files[id].in_use = 1;
     g_files[id].writable = 1;
@@ -637,9 +654,11 @@ int nc_open(const char *path, int mode, int *ncidp)
     id = alloc_slot();
     if (id < 0) return NC_ENFILE;
     fp = fopen(path, (mode & NC_WRITE) ? "r+b" : "rb");
-    if (!fp) return NC_EIO;
+    if (!fp) {
+        release(&g_files[id]);
+        return NC_EIO;
+    }
     f = &g_files[id];
-    memset(f, 0, sizeof(*f));
     f->fp = fp;
     f->in_use = 1;
     f->writable = (mode & NC_WRITE) != 0;

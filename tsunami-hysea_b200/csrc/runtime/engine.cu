@@ -16,6 +16,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -80,8 +84,11 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
 // DevScenario
 // ---------------------------------------------------------------------------
 
+DevScenario::DevScenario() = default;
+
 DevScenario::~DevScenario()
 {
+    pipe.reset();   // joins the writer before the buffers go
     if (fields) cudaFreeAsync(fields, ast);
     if (rows) cudaFreeAsync(rows, ast);
     if (def) cudaFreeAsync(def, ast);
@@ -375,18 +382,235 @@ int DevScenario::extract(int field, float *host_out, cudaStream_t st)
     return THY_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Asynchronous delivery of snapshots and gauge samples.  The reference
+// extracts, copies (blocking) and writes each snapshot inside its time loop
+// (src/GPU/ShallowWater.cu:398-421), so the GPU waits for the host.  Here
+// the extraction kernels go on the stepping stream (they read exactly the
+// state of that step, before the next steps are enqueued), the copy into a
+// page-locked host slot goes on a copy stream, and one writer thread hands
+// the slots to the caller's callbacks in event order while the GPU steps
+// on.  Snapshots use two slots of 3 fields (the first is d_out), gauge
+// samples eight slots of 4 floats per gauge; a producer that finds no free
+// slot waits for the writer.
+// ---------------------------------------------------------------------------
+class OutputPipe {
+public:
+    static constexpr int kSnapSlots = 2, kTsSlots = 8;
+
+    ~OutputPipe()
+    {
+        drain();
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            stop_ = true;
+        }
+        cv_.notify_all();
+        if (writer_.joinable()) writer_.join();
+        for (int k = 0; k < kSnapSlots; k++) {
+            if (snap_ready_[k]) cudaEventDestroy(snap_ready_[k]);
+            if (snap_copied_[k]) cudaEventDestroy(snap_copied_[k]);
+        }
+        for (int k = 0; k < kTsSlots; k++) {
+            if (ts_ready_[k]) cudaEventDestroy(ts_ready_[k]);
+            if (ts_copied_[k]) cudaEventDestroy(ts_copied_[k]);
+        }
+        if (d_snap1_) cudaFreeAsync(d_snap1_, alloc_st_);
+        if (d_ts_) cudaFreeAsync(d_ts_, alloc_st_);
+        cudaFreeHost(h_snap_);
+        cudaFreeHost(h_ts_);
+        if (copy_st_) cudaStreamDestroy(copy_st_);
+    }
+
+    int init(DevScenario *s, const thy_outputs *o, cudaStream_t st)
+    {
+        s_ = s;
+        o_ = o;
+        alloc_st_ = st;
+        n_ = (size_t)s->nx * s->ny;
+        np_ = (int)s->cells.size();
+        THY_CK(cudaStreamCreateWithFlags(&copy_st_, cudaStreamNonBlocking));
+        if (o && o->on_snapshot && s->save_nc >= 0.0) {
+            THY_CK(cudaMallocAsync(&d_snap1_, 3 * n_ * sizeof(float), st));
+            THY_CK(cudaMallocHost(&h_snap_, kSnapSlots * 3 * n_ * sizeof(float)));
+            for (int k = 0; k < kSnapSlots; k++) {
+                THY_CK(cudaEventCreateWithFlags(&snap_ready_[k], cudaEventDisableTiming));
+                THY_CK(cudaEventCreateWithFlags(&snap_copied_[k], cudaEventDisableTiming));
+            }
+        }
+        if (np_ > 0) {
+            THY_CK(cudaMallocAsync(&d_ts_, kTsSlots * 4 * (size_t)np_ * sizeof(float), st));
+            THY_CK(cudaMallocHost(&h_ts_, kTsSlots * 4 * (size_t)np_ * sizeof(float)));
+            for (int k = 0; k < kTsSlots; k++) {
+                THY_CK(cudaEventCreateWithFlags(&ts_ready_[k], cudaEventDisableTiming));
+                THY_CK(cudaEventCreateWithFlags(&ts_copied_[k], cudaEventDisableTiming));
+            }
+        }
+        writer_ = std::thread([this] { run(); });
+        return THY_OK;
+    }
+
+    bool snapshots_on() const { return h_snap_ != nullptr; }
+
+    // Extracts eta, ux, uy of the current state into a free slot and queues its delivery.
+    int snapshot(int index, double time_s, cudaStream_t st)
+    {
+        const int k = acquire(snap_busy_, kSnapSlots);
+        float *d = (k == 0) ? s_->d_out : d_snap1_;
+        for (int f = 0; f < 3; f++)
+            launch_extract(&s_->desc, kFieldEta + f, s_->hctl.parity, d + f * n_, s_->Hs, s_->Qs, s_->Hmin, st);
+        THY_CK(cudaGetLastError());
+        THY_CK(cudaEventRecord(snap_ready_[k], st));
+        THY_CK(cudaStreamWaitEvent(copy_st_, snap_ready_[k], 0));
+        THY_CK(cudaMemcpyAsync(h_snap_ + k * 3 * n_, d, 3 * n_ * sizeof(float), cudaMemcpyDeviceToHost, copy_st_));
+        THY_CK(cudaEventRecord(snap_copied_[k], copy_st_));
+        push(Job{0, index, time_s, k});
+        return THY_OK;
+    }
+
+    // Samples the gauges of the current state into a free slot and queues its delivery.
+    int gauges(int index, double time_s, cudaStream_t st)
+    {
+        const int k = acquire(ts_busy_, kTsSlots);
+        float *d = d_ts_ + k * 4 * (size_t)np_;
+        launch_gauges(&s_->desc, s_->hctl.parity, s_->d_cells, np_, d, s_->Hs, s_->Qs, s_->Hmin, st);
+        THY_CK(cudaGetLastError());
+        THY_CK(cudaEventRecord(ts_ready_[k], st));
+        THY_CK(cudaStreamWaitEvent(copy_st_, ts_ready_[k], 0));
+        THY_CK(cudaMemcpyAsync(h_ts_ + k * 4 * (size_t)np_, d, 4 * (size_t)np_ * sizeof(float),
+                               cudaMemcpyDeviceToHost, copy_st_));
+        THY_CK(cudaEventRecord(ts_copied_[k], copy_st_));
+        push(Job{1, index, time_s, k});
+        return THY_OK;
+    }
+
+    // Waits until every queued delivery has been handed to the callbacks.
+    int drain()
+    {
+        std::unique_lock<std::mutex> lk(m_);
+        cv_.wait(lk, [this] { return q_.empty() && !busy_; });
+        return error_;
+    }
+
+private:
+    struct Job {
+        int kind;     // 0 snapshot, 1 gauges
+        int index;
+        double time;
+        int slot;
+    };
+
+    int acquire(bool *busy, int n)
+    {
+        std::unique_lock<std::mutex> lk(m_);
+        for (;;) {
+            for (int k = 0; k < n; k++)
+                if (!busy[k]) {
+                    busy[k] = true;
+                    return k;
+                }
+            cv_.wait(lk);
+        }
+    }
+
+    void push(const Job &j)
+    {
+        {
+            std::lock_guard<std::mutex> lk(m_);
+            q_.push_back(j);
+        }
+        cv_.notify_all();
+    }
+
+    void run()
+    {
+        for (;;) {
+            Job j;
+            {
+                std::unique_lock<std::mutex> lk(m_);
+                cv_.wait(lk, [this] { return stop_ || !q_.empty(); });
+                if (q_.empty()) return;
+                j = q_.front();
+                q_.pop_front();
+                busy_ = true;
+            }
+            deliver(j);
+            {
+                std::lock_guard<std::mutex> lk(m_);
+                (j.kind == 0 ? snap_busy_ : ts_busy_)[j.slot] = false;
+                busy_ = false;
+            }
+            cv_.notify_all();
+        }
+    }
+
+    void deliver(const Job &j)
+    {
+        if (j.kind == 0) {
+            if (cudaEventSynchronize(snap_copied_[j.slot]) != cudaSuccess) {
+                set_error();
+                return;
+            }
+            const float *h = h_snap_ + j.slot * 3 * n_;
+            o_->on_snapshot(o_->user, j.index, j.time, h, h + n_, h + 2 * n_);
+            return;
+        }
+        if (cudaEventSynchronize(ts_copied_[j.slot]) != cudaSuccess) {
+            set_error();
+            return;
+        }
+        const float *g = h_ts_ + j.slot * 4 * (size_t)np_;
+        std::vector<float> e(np_), ux(np_), uy(np_);
+        for (int i = 0; i < np_; i++) {
+            e[i] = g[4 * i];
+            ux[i] = g[4 * i + 1];
+            uy[i] = g[4 * i + 2];
+            if (s_->cells[i] >= 0) {
+                s_->ts_min[i] = (s_->ts_min[i] < e[i]) ? s_->ts_min[i] : e[i];
+                s_->ts_max[i] = (e[i] < s_->ts_max[i]) ? s_->ts_max[i] : e[i];
+            }
+        }
+        if (o_ && o_->on_series) o_->on_series(o_->user, j.index, j.time, e.data(), ux.data(), uy.data());
+    }
+
+    void set_error()
+    {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(m_);
+        error_ = THY_ERR_CUDA;
+    }
+
+    DevScenario *s_ = nullptr;
+    const thy_outputs *o_ = nullptr;
+    cudaStream_t alloc_st_ = nullptr, copy_st_ = nullptr;
+    size_t n_ = 0;
+    int np_ = 0;
+    float *d_snap1_ = nullptr, *d_ts_ = nullptr, *h_snap_ = nullptr, *h_ts_ = nullptr;
+    cudaEvent_t snap_ready_[kSnapSlots] = {}, snap_copied_[kSnapSlots] = {};
+    cudaEvent_t ts_ready_[kTsSlots] = {}, ts_copied_[kTsSlots] = {};
+    bool snap_busy_[kSnapSlots] = {}, ts_busy_[kTsSlots] = {};
+    std::thread writer_;
+    std::mutex m_;
+    std::condition_variable cv_;
+    std::deque<Job> q_;
+    bool stop_ = false, busy_ = false;
+    int error_ = THY_OK;
+};
+
+int DevScenario::open_outputs(const thy_outputs *o, cudaStream_t st)
+{
+    if (pipe) return THY_OK;
+    if (!o || (!(o->on_snapshot && save_nc >= 0.0) && cells.empty())) return THY_OK;
+    pipe.reset(new OutputPipe());
+    return pipe->init(this, o, st);
+}
+
 int DevScenario::snapshot(const thy_outputs *o, cudaStream_t st)
 {
-    const size_t n = (size_t)nx * ny;
+    int rc;
     if (o && o->on_snapshot) {
-        std::vector<float> buf(3 * n);
-        for (int k = 0; k < 3; k++) {
-            launch_extract(&desc, kFieldEta + k, hctl.parity, d_out + k * n, Hs, Qs, Hmin, st);
-        }
-        THY_CK(cudaGetLastError());
-        THY_CK(cudaMemcpyAsync(buf.data(), d_out, 3 * n * sizeof(float), cudaMemcpyDeviceToHost, st));
-        THY_CK(cudaStreamSynchronize(st));
-        o->on_snapshot(o->user, snapshots, hctl.t * Ts, buf.data(), buf.data() + n, buf.data() + 2 * n);
+        if ((rc = open_outputs(o, st))) return rc;
+        if (pipe && pipe->snapshots_on() && (rc = pipe->snapshot(snapshots, hctl.t * Ts, st))) return rc;
     }
     snapshots++;
     return THY_OK;
@@ -394,23 +618,10 @@ int DevScenario::snapshot(const thy_outputs *o, cudaStream_t st)
 
 int DevScenario::sample_gauges(const thy_outputs *o, cudaStream_t st)
 {
-    const int np = (int)cells.size();
-    if (np > 0) {
-        std::vector<float> g(4 * (size_t)np), e(np), ux(np), uy(np);
-        launch_gauges(&desc, hctl.parity, d_cells, np, d_gauge, Hs, Qs, Hmin, st);
-        THY_CK(cudaGetLastError());
-        THY_CK(cudaMemcpyAsync(g.data(), d_gauge, g.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
-        THY_CK(cudaStreamSynchronize(st));
-        for (int i = 0; i < np; i++) {
-            e[i] = g[4 * i];
-            ux[i] = g[4 * i + 1];
-            uy[i] = g[4 * i + 2];
-            if (cells[i] >= 0) {
-                ts_min[i] = (ts_min[i] < e[i]) ? ts_min[i] : e[i];
-                ts_max[i] = (e[i] < ts_max[i]) ? ts_max[i] : e[i];
-            }
-        }
-        if (o && o->on_series) o->on_series(o->user, series, hctl.t * Ts, e.data(), ux.data(), uy.data());
+    int rc;
+    if (!cells.empty()) {
+        if ((rc = open_outputs(o, st))) return rc;
+        if (pipe && (rc = pipe->gauges(series, hctl.t * Ts, st))) return rc;
     }
     series++;
     return THY_OK;
@@ -418,8 +629,10 @@ int DevScenario::sample_gauges(const thy_outputs *o, cudaStream_t st)
 
 int DevScenario::finish(const thy_outputs *o, cudaStream_t st)
 {
-    if (!o) return THY_OK;
     int rc;
+    // every snapshot and gauge sample is delivered before the final fields
+    if (pipe && (rc = pipe->drain())) return rc;
+    if (!o) return THY_OK;
     if (o->max_height && (rc = extract(kFieldMaxHeight, o->max_height, st))) return rc;
     if (o->arrival && (rc = extract(kFieldArrival, o->arrival, st))) return rc;
     if (o->deformed_bathy && (rc = extract(kFieldDeformed, o->deformed_bathy, st))) return rc;

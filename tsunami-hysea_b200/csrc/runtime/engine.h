@@ -32,6 +32,8 @@ const char *last_error_text();
 // Okada scratch when it has faults).
 size_t scenario_bytes(int nx, int ny, bool has_faults);
 
+class OutputPipe;   // asynchronous snapshot / gauge delivery (engine.cu)
+
 // One scenario on the device.
 struct DevScenario {
     int nx = 0, ny = 0, pitch = 0;
@@ -67,8 +69,10 @@ struct DevScenario {
     int snapshots = 0, series = 0;
     std::vector<float> ts_min, ts_max;
     double first_dt_s = 0;
+    std::unique_ptr<OutputPipe> pipe;   // created at the first snapshot / gauge sample
 
     long long units() const { return (long long)desc.tiles_x * ((ny + kHalfRows - 1) / kHalfRows); }   // work units
+    DevScenario();
     ~DevScenario();
     int setup(const thy_problem *p, cudaStream_t st);   // allocate, upload, initial dt
     int upload_ctl(cudaStream_t st);
@@ -77,6 +81,7 @@ struct DevScenario {
     cudaError_t invalidate_tile_minima(cudaStream_t st);
     int encode_tensor_maps(cudaStream_t st);
     int extract(int field, float *host_out, cudaStream_t st);
+    int open_outputs(const thy_outputs *o, cudaStream_t st);
     int snapshot(const thy_outputs *o, cudaStream_t st);
     int sample_gauges(const thy_outputs *o, cudaStream_t st);
     int finish(const thy_outputs *o, cudaStream_t st);
