@@ -127,8 +127,8 @@ class PinnedOutputs:
     """Page-locked output fields for repeated runs of one grid (thysea.run's
     `out`): allocated and registered once, reused by every run."""
 
-    def __init__(self, prep: "Prepared"):
-        ny, nx = int(prep.c.ny), int(prep.c.nx)
+    def __init__(self, prep: Optional["Prepared"] = None, shape: Optional[tuple] = None):
+        ny, nx = (int(prep.c.ny), int(prep.c.nx)) if prep is not None else (int(shape[0]), int(shape[1]))
         self.fields = {k: np.empty((ny, nx), np.float32) for k in OUTPUT_FIELDS}
         L = _ffi.lib()
         self._reg = []
