@@ -479,7 +479,9 @@ def run_batched(a, dist):
         rr = np.random.default_rng(int(seeds[k]))
         p = synth.Problem(name=f"req{k:04d}", lon=lon, lat=lat, z=z, faults=[synth.random_fault(lon, lat, z, rr)],
                           sim_time=float(t_sim[k]))
-        return thysea.Prepared(p).pin()
+        # not page-locked: registering hundreds of MB from the preparing
+        # threads would hold the driver while the stepping loop issues work
+        return thysea.Prepared(p)
 
     lead = 4.0   # seconds of look-ahead for the preparing threads
     pool = cf.ThreadPoolExecutor(max_workers=4)

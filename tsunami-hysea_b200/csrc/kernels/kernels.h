@@ -34,8 +34,9 @@ struct StepLaunch {
 constexpr int kLaunchesPerStep = 6;
 void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st);
 void launch_initial_dt(const StepLaunch &L, cudaStream_t st);
-// every work item on the general list (after the host changed a state)
-void launch_lists_all_general(const StepLaunch &L, cudaStream_t st);
+// lists for the current states of the work list's scenarios (from the host,
+// before a chunk: after the work list or a state changed)
+void launch_lists_current(const StepLaunch &L, cudaStream_t st);
 int deep_blocks_per_sm(int phase);
 
 // init.cu: double-precision host state (reference layout, dimensionless) to

@@ -502,15 +502,18 @@ __device__ __forceinline__ const int *deep_items(const int *lists) { return list
 __device__ __forceinline__ const int *general_items(const int *lists, int cap) { return lists + 2 + cap; }
 
 // Splits the work units into deep and general lists (dry units go to
-// neither) for the state the next phase reads: after phase 1 of a running
-// scenario that is the state phase 1 produced (summaries at parity^1), which
-// phase 2 of this step and phase 1 of the next step both read; for a scenario
-// that is not running it is the state at its current parity.  all_general
-// (after the host changed a state) puts every unit on the general list.
-// Units below the grid (the lower half of a last tile row of <= 16 rows) are
-// not listed.  The counts are zeroed before the launch.
+// neither) for the state the next phase reads.  In the step (before_step = 0,
+// after phase 1): for a running scenario that is the state phase 1 produced
+// (summaries at parity^1), which phase 2 of this step and phase 1 of the next
+// step both read, and the dry counts advance; for a scenario that is not
+// running it is the state at its current parity.  From the host before a
+// chunk (before_step = 1, the work list or a state changed): the state at the
+// current parity for every scenario, dry counts unchanged; a state the host
+// changed has unknown (NaN) summaries, so its units are general.  Units below
+// the grid (the lower half of a last tile row of <= 16 rows) are not listed.
+// The counts are zeroed before the launch.
 __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int all_general)
+                                const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int before_step)
 {
     const int n = 2 * *nwork_ptr;
     const int lane = threadIdx.x & 31;
@@ -523,9 +526,9 @@ __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2
             const int ty = item.y / s.tiles_x, tx = item.y - ty * s.tiles_x;
             const int uy = 2 * ty + (u & 1);
             listed = uy * kHalfRows < s.ny;
-            if (listed && !all_general) {
+            if (listed) {
                 ScenarioCtl *ctl = s.ctl;
-                const bool running = ctl->status == kRunning;
+                const bool running = !before_step && ctl->status == kRunning;
                 const int par = running ? (ctl->parity ^ 1) : ctl->parity;
                 const UnitSum *sum = s.usum[par];
                 deep = unit_deep(s, sum, tx, uy);
@@ -1156,7 +1159,7 @@ void launch_initial_dt(const StepLaunch &L, cudaStream_t st)
     step_kernel<0><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap);
 }
 
-void launch_lists_all_general(const StepLaunch &L, cudaStream_t st)
+void launch_lists_current(const StepLaunch &L, cudaStream_t st)
 {
     cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
     classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 1);

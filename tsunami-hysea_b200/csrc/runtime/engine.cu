@@ -731,13 +731,14 @@ int Batch::detach(DevScenario *s)
     return THY_OK;
 }
 
-int Batch::update()
+int Batch::update(const std::vector<char> *selected)
 {
     std::vector<ScenarioDev> table(capacity);
     std::vector<int2> work;
     for (int i = 0; i < capacity; i++) {
         if (!members[i]) continue;
         table[i] = members[i]->desc;
+        if (selected && !(*selected)[i]) continue;
         for (int t = 0; t < members[i]->desc.ntiles; t++) work.push_back(make_int2(i, t));
     }
     if ((int)work.size() > work_capacity) {
@@ -833,7 +834,7 @@ StepLaunch Batch::params() const
 
 int Batch::reset_lists()
 {
-    launch_lists_all_general(params(), st);
+    launch_lists_current(params(), st);
     THY_CK(cudaGetLastError());
     return THY_OK;
 }

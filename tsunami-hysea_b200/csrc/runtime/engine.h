@@ -117,13 +117,15 @@ struct Batch {
     int init(int capacity, int max_work, cudaStream_t stream);
     int attach(DevScenario *s);      // gives s a control slot
     int detach(DevScenario *s);
-    int update();                     // upload the member table and the work list, reset the lists
+    // upload the member table and the work list (of the members with
+    // selected[slot] != 0, all of them without a selection) and classify
+    int update(const std::vector<char> *selected = nullptr);
     int capture();                    // (re)capture the step graph for the current capacity
     int rebuild();                    // update(), and capture() when there is no graph yet
     int initial_dt_of(DevScenario *s);   // initial dt of one member (phase 0 over its units only)
     int run_chunk(bool timed);       // one graph launch + control download (synchronous)
     StepLaunch params() const;
-    int reset_lists();               // all items general: after the host changed a member's state
+    int reset_lists();               // classify again: after the host changed a member's state
 };
 
 int ensure_device();

@@ -54,6 +54,7 @@ struct thy_server {
     std::deque<thy::Request> queue;
     std::vector<thy::Active *> slots;     // by batch slot
     bool members_changed = false;
+    std::vector<char> selected;           // by batch slot: stepped in the last chunk (its work list)
     thy_server_stats stats{};
 };
 
@@ -249,8 +250,10 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
     // Work budget of the chunk: the resident scenarios with the least
     // remaining work (cells x remaining steps at the current dt) are stepped
     // until their cells reach chunk_cells; the others wait (status idle on
-    // the device, so every kernel skips them).  Small requests are batched,
-    // a large one runs nearly alone, and no request's arithmetic changes.
+    // the device, and their tiles are not on the chunk's work list).  Small
+    // requests are batched, a large one runs nearly alone, and no request's
+    // arithmetic changes.
+    std::vector<char> sel(cap, 0);
     if (any_running) {
         std::vector<std::pair<double, int>> order;
         for (int i = 0; i < cap; i++) {
@@ -268,6 +271,7 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             DevScenario &s = *a->s;
             const bool step = S->chunk_cells < 0 || taken < (double)S->chunk_cells;
             if (step) taken += (double)s.nx * s.ny;
+            sel[e.second] = step ? 1 : 0;
             const int want = step ? kRunning : kIdle;
             if (s.hctl.status != want || a->deferred == step) {
                 s.hctl.status = want;
@@ -276,9 +280,12 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             }
         }
     }
-    if (S->members_changed) {
-        if ((rc = S->b.rebuild())) return rc;   // table + work list (+ lists reset)
+    if (S->members_changed || sel != S->selected) {
+        // table + the work list of the stepped scenarios, classified for their current states
+        if ((rc = S->b.update(&sel))) return rc;
+        if (!S->b.gexec && (rc = S->b.capture())) return rc;   // the list outgrew its capacity
         S->members_changed = false;
+        S->selected = sel;
     } else if (state_changed) {
         if ((rc = S->b.reset_lists())) return rc;
     }
