@@ -148,56 +148,60 @@ extern "C" int thy_load_problem_file(const char *txt_path, thy_raw_owned **out)
         return THY_ERR_INVALID;
     };
     r.series_time = -1.0;
-    next_value(in, R->name);
-    next_value(in, topo);
+    // every value up to H is required; a file that ends early is refused
+    auto need = [&](bool ok, const char *what) { return ok ? 0 : (fail(std::string("the problem file ends before ") + what), 1); };
+    if (need(next_value(in, R->name), "the problem name") || need(next_value(in, topo), "the bathymetry file"))
+        return THY_ERR_INVALID;
     if (!file_exists(dir + topo)) return fail("File '" + dir + topo + "' not found");
-    next_value(in, init);
+    if (need(next_value(in, init), "the initialization type")) return THY_ERR_INVALID;
     if (init != 0 && init != 1) return fail("The initialization flag should be 0 or 1");
     if (init == 0) {
-        next_value(in, est);
+        if (need(next_value(in, est), "the initial state file")) return THY_ERR_INVALID;
         if (!file_exists(dir + est)) return fail("File '" + dir + est + "' not found");
     } else {
-        next_value(in, r.nfaults);
+        if (need(next_value(in, r.nfaults), "the number of faults")) return THY_ERR_INVALID;
         if (r.nfaults < 1 || r.nfaults > kMaxFaults) return fail("The number of faults should be between 1 and 5000");
         R->faults.resize(10 * (size_t)r.nfaults);
         for (int i = 0; i < r.nfaults; i++) {
             std::istringstream iss(next_line(in));
-            for (int k = 0; k < 10; k++) iss >> R->faults[10 * i + k];
+            for (int k = 0; k < 10; k++)
+                if (!(iss >> R->faults[10 * i + k])) return fail("a fault line has fewer than 10 values");
         }
-        next_value(in, r.crop_flag);
+        if (need(next_value(in, r.crop_flag), "the cropping flag")) return THY_ERR_INVALID;
         if (r.crop_flag < 0 || r.crop_flag > 2) return fail("The cropping flag should be 0, 1 or 2");
-        if (r.crop_flag == 1 || r.crop_flag == 2) next_value(in, r.crop_value);
+        if ((r.crop_flag == 1 || r.crop_flag == 2) && need(next_value(in, r.crop_value), "the cropping value"))
+            return THY_ERR_INVALID;
     }
-    next_value(in, R->prefix);
+    if (need(next_value(in, R->prefix), "the output prefix")) return THY_ERR_INVALID;
     if (read_grd(dir + topo, R->lon, R->lat, R->z)) return fail("cannot read the bathymetry file '" + dir + topo + "'");
     r.nx = (int)R->lon.size();
     r.ny = (int)R->lat.size();
     if (r.nx < 2 || r.ny < 2) return fail("Mesh size too small. The number of rows and columns should be >= 2");
-    next_value(in, levels);
+    if (need(next_value(in, levels), "the number of levels")) return THY_ERR_INVALID;
     if (levels != 1) return fail("The number of levels should be 1");
-    for (int k = 0; k < 4; k++) next_value(in, r.borders[k]);
+    for (int k = 0; k < 4; k++)
+        if (need(next_value(in, r.borders[k]), "the four borders")) return THY_ERR_INVALID;
     for (int k = 0; k < 4; k++)
         if (!border_ok(r.borders[k])) return fail("The boundary conditions should be -1, 1 or 2");
     if (std::fabs(r.borders[0] - 2.0) < kEps || std::fabs(r.borders[1] - 2.0) < kEps)
         return fail("Periodic boundary conditions are only supported for left and right borders");
     if ((std::fabs(r.borders[2] - 2.0) < kEps) != (std::fabs(r.borders[3] - 2.0) < kEps))
         return fail("Both left and right borders should have periodic boundary conditions");
-    next_value(in, r.sim_time);
-    next_value(in, r.save_time);
-    next_value(in, read_points);
+    if (need(next_value(in, r.sim_time), "the simulation time") ||
+        need(next_value(in, r.save_time), "the NetCDF saving time") ||
+        need(next_value(in, read_points), "the points flag"))
+        return THY_ERR_INVALID;
     if (read_points == 1) {
-        next_value(in, pts_file);
-        next_value(in, r.series_time);
+        if (need(next_value(in, pts_file), "the points file") ||
+            need(next_value(in, r.series_time), "the time-series saving time"))
+            return THY_ERR_INVALID;
         if (!file_exists(dir + pts_file)) return fail("File '" + dir + pts_file + "' not found");
     }
-    next_value(in, r.cfl);
-    next_value(in, r.eps_h);
-    next_value(in, r.hpos);
-    next_value(in, r.stability);
-    next_value(in, r.manning);
-    next_value(in, r.vmax);
-    next_value(in, r.L);
-    next_value(in, r.H);
+    if (need(next_value(in, r.cfl), "CFL") || need(next_value(in, r.eps_h), "epsilon h") ||
+        need(next_value(in, r.hpos), "the 2s+WAF threshold") || need(next_value(in, r.stability), "the stability coefficient") ||
+        need(next_value(in, r.manning), "Manning") || need(next_value(in, r.vmax), "the maximum velocity") ||
+        need(next_value(in, r.L), "L") || need(next_value(in, r.H), "H"))
+        return THY_ERR_INVALID;
     r.dif_at = r.eps_h;   // default when the line is absent (src/Problema.cxx:327)
     next_value(in, r.dif_at);
     if (init == 0) {
