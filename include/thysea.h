@@ -114,6 +114,14 @@ typedef struct thy_outputs {
     void *user;
 } thy_outputs;
 
+/* Warp tiling of the stepping kernels: a variant index 0..2 per kernel
+   (row groups of 4 column-strip warps per work unit: deep phase 1 {3, 2, 4},
+   deep phase 2 {2, 1, 3}, general {2, 1, 4}; 0 is the default).  No result
+   depends on the tiling; the autotuner picks one per device and work size. */
+typedef struct thy_tiling {
+    int deep1, deep2, general;
+} thy_tiling;
+
 typedef struct thy_stats {
     long long steps;          /* time steps taken */
     double final_time_s;      /* simulated time reached */
@@ -128,6 +136,8 @@ typedef struct thy_stats {
     double setup_seconds;     /* device set-up before the loop: upload, metrics, graph capture */
     double output_seconds;    /* extraction and download of the output fields after the loop */
     double total_seconds;     /* the whole call, release of the device buffers included */
+    thy_tiling tiling;        /* the warp tiling of the loop's last chunk */
+    long long tune_samples;   /* chunks of the loop timed for the autotuner */
 } thy_stats;
 
 /* Library / device. */
@@ -210,7 +220,23 @@ long long thy_session_launches(const thy_session *s);   /* stepping kernels laun
    the deep-water kernels, and skipped as settled dry land */
 int thy_session_tiles(const thy_session *s, long long *tiles, long long *deep_tiles, long long *dry_tiles);
 double thy_session_time(const thy_session *s);    /* simulated time (s) */
+/* step (real steps of the run) until the autotuner has decided the tiling
+   for this problem's work size, at most max_steps; *steps_done: steps taken */
+int thy_session_tune(thy_session *s, long long max_steps, long long *steps_done);
+int thy_session_tiling(const thy_session *s, thy_tiling *t);   /* tiling of the last chunk */
 void thy_session_close(thy_session *s);
+
+/* Autotuner of the warp tilings.  Every full chunk of a run (of any entry
+   point) is timed as one sample of the tiling it ran with; the search, per
+   device and work size (ceil log2 of the work units a step visits), is
+   coordinate descent over deep phase 2, deep phase 1 and the general kernel.
+   Environment: THY_TILING="d1,d2,g" forces a tiling, THY_TUNE=0 keeps the
+   default, THY_TUNE_CACHE=<file> keeps decided tilings across processes. */
+int thy_tiling_force(const thy_tiling *t);          /* NULL: autotune again */
+/* 1 when the tiling for `units` work units per step is decided on the current
+   device (*best set), 0 while tuning (*best: the incumbent) */
+int thy_tiling_tuned(long long units, thy_tiling *best);
+void thy_tuner_clear(void);                         /* forget every decision of this process */
 
 /* Multi-scenario runtime (batched and serving use): scenarios submitted at
    any time are admitted in order under an HBM budget and stepped together -

@@ -1,0 +1,76 @@
+"""Warp tilings and their autotuner on the GPU: every tiling of the stepping
+kernels gives bitwise the same results (a tiling only changes which warp
+computes which cells), a run whose chunks the autotuner switches between
+tilings gives the default tiling's results, and the tuner reaches a decision
+on a session."""
+import numpy as np
+import pytest
+
+import thysea
+from thysea import synth
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("max_height", "arrival", "eta", "ux", "uy")
+TILINGS = [(0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (0, 2, 0), (0, 0, 1), (0, 0, 2), (2, 1, 2), (1, 2, 1)]
+
+
+def _problem():
+    # deep ocean, shelf, coast and land (deep, general and dry units), with a
+    # partial last tile in both directions
+    p = synth.single_large(n=352, seed=31, sim_time=900.0)
+    p.name = "tiling"
+    return p
+
+
+def _run(prep):
+    r = thysea.run(prep, snapshots=False, series=False)
+    return {k: r[k].copy() for k in FIELDS}, r
+
+
+@pytest.fixture
+def untuned():
+    thysea.clear_tuner()
+    yield
+    thysea.force_tiling(None)
+    thysea.clear_tuner()
+
+
+def test_every_tiling_gives_the_same_results(gpu, untuned):
+    prep = thysea.Prepared(_problem())
+    thysea.force_tiling((0, 0, 0))
+    ref, r0 = _run(prep)
+    assert r0["iterations"] > 100 and r0["tiling"] == (0, 0, 0) and r0["tune_samples"] == 0
+    assert r0["deep_tiles"] > 0 and r0["dry_tiles"] > 0
+    for t in TILINGS[1:]:
+        thysea.force_tiling(t)
+        got, r = _run(prep)
+        assert r["tiling"] == t and r["iterations"] == r0["iterations"]
+        for k in FIELDS:
+            assert np.array_equal(got[k], ref[k], equal_nan=True), (t, k)
+
+
+def test_autotuned_run_gives_the_default_results(gpu, untuned):
+    prep = thysea.Prepared(_problem())
+    thysea.force_tiling((0, 0, 0))
+    ref, r0 = _run(prep)
+    thysea.force_tiling(None)
+    got, r = _run(prep)   # its chunks switch tilings while the tuner samples
+    assert r["tune_samples"] > 0
+    for k in FIELDS:
+        assert np.array_equal(got[k], ref[k], equal_nan=True), k
+
+
+def test_session_tune_decides(gpu, untuned):
+    p = synth.single_large(n=640, seed=32, sim_time=3600.0)
+    s = thysea.Session(p)
+    steps = s.tune()
+    # 3 kernels x 3 candidates x 2 samples of one 16-step chunk each
+    assert 18 * 16 <= steps <= 40 * 16
+    # the key: work units one step visits (two per 112 x 32 tile)
+    units = 2 * (-(-p.nx // 112)) * (-(-p.ny // 32))
+    decided, best = thysea.tuned_tiling(units)
+    assert decided and all(0 <= v < 3 for v in best)
+    s.steps(16)
+    assert s.tiling() == best
+    s.close()

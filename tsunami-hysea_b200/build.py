@@ -32,6 +32,7 @@ CUDA_SOURCES = [
     "kernels/okada.cu",
     "runtime/engine.cu",
     "runtime/server.cu",
+    "runtime/tuner.cu",
     "runtime/okada_api.cu",
     "host/netcdf_out.cpp",
     "host/dropin.cpp",

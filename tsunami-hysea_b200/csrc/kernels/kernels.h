@@ -12,9 +12,33 @@ constexpr int kStepThreads = 128;           // 4 warps = 4 column strips per til
 constexpr int kTileX = 28 * (kStepThreads / 32);   // tile width: 28 output columns per warp
 constexpr int kTileY = 32;                  // tile height: rows one warp marches through
 
+// Warp tilings of the stepping kernels, picked per workload by the autotuner
+// (runtime/tuner.cu).  A work unit is always kTileX x kHalfRows cells, each
+// of its four column strips marched by warps; a tiling says into how many row
+// groups a unit's rows are split (warps per CTA = 4 x groups) and how many
+// CTAs an SM keeps resident.  Every cell's arithmetic is the same under every
+// tiling (a warp recomputes the y edge above its first row from the same
+// inputs), so results do not depend on the tiling.  Variant 0 is the default.
+constexpr int kTilingVariants = 3;
+struct Tiling {
+    int deep1 = 0, deep2 = 0, general = 0;   // variant of deep phase 1, deep phase 2, the general kernel
+    bool operator==(const Tiling &o) const { return deep1 == o.deep1 && deep2 == o.deep2 && general == o.general; }
+    bool operator!=(const Tiling &o) const { return !(*this == o); }
+};
+// row groups per unit: deep phase 1 {3, 2, 4}, deep phase 2 {2, 1, 3}, general {2, 1, 4}
+__host__ __device__ constexpr int deep_ng(int phase, int v)
+{
+    return phase == 1 ? (v == 0 ? 3 : v == 1 ? 2 : 4) : (v == 0 ? 2 : v == 1 ? 1 : 3);
+}
+// resident CTAs per SM the deep kernels are compiled for: phase 1 is held to
+// two by its staging buffers; phase 2 runs three unless 12 warps a CTA need
+// more registers than three CTAs leave
+__host__ __device__ constexpr int deep_minb(int phase, int v) { return phase == 1 ? 2 : (deep_ng(2, v) == 3 ? 2 : 3); }
+__host__ __device__ constexpr int general_ng(int v) { return v == 0 ? 2 : v == 1 ? 1 : 4; }
+
 // step.cu
 cudaError_t configure_step_kernels();
-int step_blocks_per_sm();
+int step_blocks_per_sm(int general_variant);
 // Launch parameters of the stepping kernels of a batch.
 struct StepLaunch {
     const ScenarioDev *scen;   // scenario table (nslots entries)
@@ -26,6 +50,7 @@ struct StepLaunch {
     int deep_grid[2];          // persistent deep kernel grids, phase 1 and 2
     int classify_grid;
     int nslots;
+    Tiling tiling;
 };
 
 // The kLaunchesPerStep launches of a time step, in order: 0 deep phase 1,
@@ -37,7 +62,7 @@ void launch_initial_dt(const StepLaunch &L, cudaStream_t st);
 // lists for the current states of the work list's scenarios (from the host,
 // before a chunk: after the work list or a state changed)
 void launch_lists_current(const StepLaunch &L, cudaStream_t st);
-int deep_blocks_per_sm(int phase);
+int deep_blocks_per_sm(int phase, int variant);
 
 // init.cu: double-precision host state (reference layout, dimensionless) to
 // the FP32 device state; metrics initialised as in src/GPU/ShallowWater.cu:305-309

@@ -47,9 +47,7 @@ constexpr int STRIPS = kStepThreads / 32;   // column strips of a tile
 constexpr int OUTW = 28;              // output columns per strip
 constexpr int TY = kTileY;            // output rows per tile
 static_assert(kTileX == STRIPS * OUTW, "tile width = strips x 28 columns");
-constexpr int GWARPS = 2 * STRIPS;    // general kernel: every strip of a unit in two row groups
-constexpr int GNT = 32 * GWARPS;
-constexpr int GROWS = kHalfRows / 2;  // rows a general-kernel warp marches
+static_assert(STRIPS == 4, "deep and general kernels: 4 column-strip warps per row group");
 
 // one cell of a lane's column: depth, surface elevation, still-water depth, discharges
 struct Cell {
@@ -451,12 +449,10 @@ __device__ __forceinline__ void tmap_acquire(const TmaMap *map)
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
 }
 
-// Warps of a deep-kernel CTA: 4 column strips x row groups.  Phase 1 (two
-// CTAs per SM: its double-buffered staging is larger) uses 3 row groups so
-// that 24 warps per SM hide the latency; phase 2 uses 2 at three CTAs per SM.
-__host__ __device__ constexpr int deep_groups(int phase) { return phase == 1 ? 3 : 2; }
-__host__ __device__ constexpr int deep_warps(int phase) { return 4 * deep_groups(phase); }
-__host__ __device__ constexpr int deep_threads(int phase) { return 32 * deep_warps(phase); }
+// Warps of a deep-kernel CTA: 4 column strips x NG row groups (the tiling's
+// variant: by default phase 1, two CTAs per SM as its double-buffered staging
+// is larger, uses 3 row groups so that 24 warps per SM hide the latency;
+// phase 2 uses 2 at three CTAs per SM).
 constexpr int SPLANE = (kStageRows * kStageW + 31) / 32 * 32;   // floats per staged plane (128-byte multiple)
 constexpr int DPLANE = kHalfRows * kTileX;          // floats per staged diagnostics plane
 constexpr uint32_t kStateBytes = kStageRows * kStageW * 4;
@@ -478,9 +474,9 @@ struct DeepRow {
     float pad[3];
 };
 __host__ __device__ constexpr size_t deep_misc_offset(int phase) { return 2 * deep_stage_bytes(phase); }
-static size_t deep_smem_bytes(int phase)
+static size_t deep_smem_bytes(int phase, int ng)
 {
-    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + 2 * deep_warps(phase) * sizeof(float);
+    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + 2 * 4 * ng * sizeof(float);
 }
 
 // one cell of a staged row (shared memory; the depth is formed here)
@@ -640,8 +636,8 @@ __device__ __forceinline__ void deep_issue(const DeepUnit &d, float *stage, uint
 // staged by TMA, the next unit's copy in flight while the current one is
 // computed.  Warp w marches its row group (w >> 2) of column strip w & 3 (28
 // output columns, lanes 2..29) with a two-row window.
-template <int PHASE>
-__global__ void __launch_bounds__(deep_threads(PHASE), PHASE == 1 ? 2 : 3) deep_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+template <int PHASE, int NG, int MINB>
+__global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                                    const int *__restrict__ lists)
 {
     extern __shared__ __align__(1024) unsigned char dsm[];
@@ -651,7 +647,7 @@ __global__ void __launch_bounds__(deep_threads(PHASE), PHASE == 1 ? 2 : 3) deep_
     DeepRow *rows = reinterpret_cast<DeepRow *>(dsm + deep_misc_offset(PHASE) + 16);
     float *red = reinterpret_cast<float *>(rows + kStageRows);   // per warp: dt, or depth min and max
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = deep_warps(PHASE), NG = deep_groups(PHASE);
+    constexpr int NW = 4 * NG;
     const int strip = warp & 3, group = warp >> 2;
     // this warp's rows of the unit: kHalfRows * group / NG .. kHalfRows * (group + 1) / NG - 1
     const int row0 = kHalfRows * group / NG, nrows = kHalfRows * (group + 1) / NG - row0;
@@ -841,14 +837,16 @@ __global__ void __launch_bounds__(deep_threads(PHASE), PHASE == 1 ? 2 : 3) deep_
     }
 }
 
-// General kernel, one work unit (half tile) per CTA iteration, 8 warps (4
-// column strips x 2 row groups): phase 0 over every unit of the work list,
-// phases 1 and 2 over the general list of the step.
-template <int PHASE>
-__global__ void __launch_bounds__(GNT) step_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+// General kernel, one work unit (half tile) per CTA iteration, 4 x NG warps
+// (4 column strips x NG row groups of kHalfRows / NG rows): phase 0 over every
+// unit of the work list, phases 1 and 2 over the general list of the step.
+template <int PHASE, int NG>
+__global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                                    const int *__restrict__ nwork_ptr, const int *__restrict__ lists,
                                                    int cap)
 {
+    constexpr int GWARPS = 4 * NG, GROWS = kHalfRows / NG;
+    static_assert(kHalfRows % NG == 0, "row groups of equal height");
     __shared__ float red[GWARPS];          // phases 0 / 2: dt per warp
     __shared__ float2 slots[9 * GWARPS];   // phase 1: unit summary per warp
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -1135,28 +1133,52 @@ __global__ void controller_kernel(const ScenarioDev *__restrict__ scen, int nslo
 }
 
 
+// One launch of deep phase PHASE / the general kernel in variant V.
+template <int PHASE, int V>
+static void launch_deep(const StepLaunch &L, cudaStream_t st)
+{
+    constexpr int NG = deep_ng(PHASE, V);
+    deep_kernel<PHASE, NG, deep_minb(PHASE, V)>
+        <<<L.deep_grid[PHASE - 1], 128 * NG, deep_smem_bytes(PHASE, NG), st>>>(L.scen, L.work, L.lists);
+}
+template <int PHASE>
+static void launch_deep_any(const StepLaunch &L, cudaStream_t st)
+{
+    switch (PHASE == 1 ? L.tiling.deep1 : L.tiling.deep2) {
+    case 1: launch_deep<PHASE, 1>(L, st); break;
+    case 2: launch_deep<PHASE, 2>(L, st); break;
+    default: launch_deep<PHASE, 0>(L, st); break;
+    }
+}
+template <int PHASE>
+static void launch_general(const StepLaunch &L, cudaStream_t st)
+{
+    switch (L.tiling.general) {
+    case 1: step_kernel<PHASE, general_ng(1)><<<L.grid, 128 * general_ng(1), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    case 2: step_kernel<PHASE, general_ng(2)><<<L.grid, 128 * general_ng(2), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    default: step_kernel<PHASE, general_ng(0)><<<L.grid, 128 * general_ng(0), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    }
+}
+
 void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
 {
     switch (k) {
-    case 0:
-        deep_kernel<1><<<L.deep_grid[0], deep_threads(1), deep_smem_bytes(1), st>>>(L.scen, L.work, L.lists);
-        break;
-    case 1: step_kernel<1><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    case 0: launch_deep_any<1>(L, st); break;
+    case 1: launch_general<1>(L, st); break;
     case 2:
         cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
         classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0);
         break;
-    case 3:
-        deep_kernel<2><<<L.deep_grid[1], deep_threads(2), deep_smem_bytes(2), st>>>(L.scen, L.work, L.lists);
-        break;
-    case 4: step_kernel<2><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    case 3: launch_deep_any<2>(L, st); break;
+    case 4: launch_general<2>(L, st); break;
     default: controller_kernel<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.scen, L.nslots); break;
     }
 }
 
+// phase 0 (initial dt) runs once per scenario: default tiling, the grid of L
 void launch_initial_dt(const StepLaunch &L, cudaStream_t st)
 {
-    step_kernel<0><<<L.grid, GNT, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap);
+    step_kernel<0, general_ng(0)><<<L.grid, 128 * general_ng(0), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap);
 }
 
 void launch_lists_current(const StepLaunch &L, cudaStream_t st)
@@ -1165,32 +1187,51 @@ void launch_lists_current(const StepLaunch &L, cudaStream_t st)
     classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 1);
 }
 
+template <int PHASE, int V>
+static cudaError_t configure_deep()
+{
+    constexpr int NG = deep_ng(PHASE, V);
+    auto *f = deep_kernel<PHASE, NG, deep_minb(PHASE, V)>;
+    cudaError_t e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deep_smem_bytes(PHASE, NG));
+    if (e) return e;
+    return cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+}
+
 cudaError_t configure_step_kernels()
 {
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(deep_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deep_smem_bytes(1))))
+    if ((e = configure_deep<1, 0>()) || (e = configure_deep<1, 1>()) || (e = configure_deep<1, 2>()) ||
+        (e = configure_deep<2, 0>()) || (e = configure_deep<2, 1>()) || (e = configure_deep<2, 2>()))
         return e;
-    if ((e = cudaFuncSetAttribute(deep_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)deep_smem_bytes(2))))
-        return e;
-    if ((e = cudaFuncSetAttribute(deep_kernel<1>, cudaFuncAttributePreferredSharedMemoryCarveout, 100))) return e;
-    return cudaFuncSetAttribute(deep_kernel<2>, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    return cudaSuccess;
 }
 
-int step_blocks_per_sm()
+// Resident CTAs per SM of the phase-2 general kernel / a deep kernel in a variant.
+int step_blocks_per_sm(int v)
 {
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2>, GNT, 0);
+    switch (v) {
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2, general_ng(1)>, 128 * general_ng(1), 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2, general_ng(2)>, 128 * general_ng(2), 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2, general_ng(0)>, 128 * general_ng(0), 0); break;
+    }
     return n;
 }
 
-int deep_blocks_per_sm(int phase)
+template <int PHASE, int V>
+static int deep_occupancy()
 {
+    constexpr int NG = deep_ng(PHASE, V);
     int n = 0;
-    if (phase == 1)
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<1>, deep_threads(1), deep_smem_bytes(1));
-    else
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<2>, deep_threads(2), deep_smem_bytes(2));
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<PHASE, NG, deep_minb(PHASE, V)>, 128 * NG,
+                                                  deep_smem_bytes(PHASE, NG));
     return n;
+}
+
+int deep_blocks_per_sm(int phase, int v)
+{
+    if (phase == 1) return v == 1 ? deep_occupancy<1, 1>() : v == 2 ? deep_occupancy<1, 2>() : deep_occupancy<1, 0>();
+    return v == 1 ? deep_occupancy<2, 1>() : v == 2 ? deep_occupancy<2, 2>() : deep_occupancy<2, 0>();
 }
 
 }  // namespace thy

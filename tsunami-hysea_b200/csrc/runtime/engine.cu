@@ -11,6 +11,7 @@
 // the scenario; later launches of the chunk do nothing for it, and the host
 // performs the event exactly at that step before resuming.
 #include "engine.h"
+#include "tuner.h"
 
 #include <cuda.h>
 
@@ -661,7 +662,7 @@ int DevScenario::finish(const thy_outputs *o, cudaStream_t st)
 
 Batch::~Batch()
 {
-    if (gexec) cudaGraphExecDestroy(gexec);
+    drop_graphs();
     if (d_table) cudaFreeAsync(d_table, st);
     if (d_work) cudaFreeAsync(d_work, st);
     if (d_nwork) cudaFreeAsync(d_nwork, st);
@@ -682,6 +683,7 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     capacity = cap;
     work_capacity = max_work;
     st = stream;
+    THY_CK(cudaGetDevice(&device));
     THY_CK(cudaMallocAsync(&d_table, cap * sizeof(ScenarioDev), st));
     THY_CK(cudaMallocAsync(&d_ctl, cap * sizeof(ScenarioCtl), st));
     THY_CK(cudaMallocHost(&h_ctl, cap * sizeof(ScenarioCtl)));
@@ -751,10 +753,7 @@ int Batch::update(const std::vector<char> *selected)
         THY_CK(cudaMallocAsync(&d_work, work_capacity * sizeof(int2), st));
         THY_CK(cudaMallocAsync(&d_work0, work_capacity * sizeof(int2), st));
         THY_CK(cudaMallocAsync(&d_lists, (2 + 4 * (size_t)work_capacity) * sizeof(int), st));
-        if (gexec) {
-            cudaGraphExecDestroy(gexec);
-            gexec = nullptr;
-        }
+        drop_graphs();
     }
     nwork = (int)work.size();
     THY_CK(cudaMemcpyAsync(d_table, table.data(), capacity * sizeof(ScenarioDev), cudaMemcpyHostToDevice, st));
@@ -764,20 +763,37 @@ int Batch::update(const std::vector<char> *selected)
     return reset_lists();
 }
 
-// Grids depend on the work-list capacity only, so the graph survives changes
-// of the member set (the kernels read the table and the lists from device
-// memory).
+void Batch::drop_graphs()
+{
+    for (auto &g : graphs) cudaGraphExecDestroy(g.second);
+    graphs.clear();
+    gexec = nullptr;
+}
+
+int Batch::use_tiling(const Tiling &t)
+{
+    if (gexec && t == tiling) return THY_OK;
+    tiling = t;
+    for (auto &g : graphs)
+        if (g.first == t) {
+            gexec = g.second;
+            return THY_OK;
+        }
+    return capture();
+}
+
+// Grids depend on the work-list capacity and the tiling only, so a graph
+// survives changes of the member set (the kernels read the table and the
+// lists from device memory).
 int Batch::capture()
 {
-    const int bps = std::max(1, step_blocks_per_sm());
-    grid = std::max(1, std::min(2 * work_capacity, device_sm_count() * bps * 8));
-    for (int ph = 0; ph < 2; ph++)
-        deep_grid[ph] =
-            std::max(1, std::min(2 * work_capacity, device_sm_count() * std::max(1, deep_blocks_per_sm(ph + 1))));
-    if (gexec) {
-        cudaGraphExecDestroy(gexec);
-        gexec = nullptr;
-    }
+    for (size_t i = 0; i < graphs.size(); i++)
+        if (graphs[i].first == tiling) {
+            cudaGraphExecDestroy(graphs[i].second);
+            graphs.erase(graphs.begin() + i);
+            break;
+        }
+    gexec = nullptr;
     // Each phase's general and deep-water kernels step disjoint tiles and
     // share only atomically updated scenario fields, so they are two
     // branches of the graph: the deep tiles fill the SMs the general
@@ -801,6 +817,7 @@ int Batch::capture()
     cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
     cudaGraphDestroy(g);
     THY_CK(e);
+    graphs.emplace_back(tiling, gexec);
     return THY_OK;
 }
 
@@ -824,9 +841,13 @@ StepLaunch Batch::params() const
     L.nwork = d_nwork;
     L.lists = d_lists;
     L.cap = 2 * work_capacity;   // lists hold work units (two per work-list entry)
-    L.grid = grid;
-    L.deep_grid[0] = deep_grid[0];
-    L.deep_grid[1] = deep_grid[1];
+    L.tiling = tiling;
+    // general kernel: a grid of 8 waves of resident CTAs striding over the
+    // list; deep kernels: persistent, one wave
+    const int sms = device_sm_count();
+    L.grid = std::max(1, std::min(2 * work_capacity, sms * std::max(1, step_blocks_per_sm(tiling.general)) * 8));
+    L.deep_grid[0] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(1, tiling.deep1))));
+    L.deep_grid[1] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(2, tiling.deep2))));
     L.classify_grid = std::max(1, std::min((2 * work_capacity + 255) / 256, 4 * device_sm_count()));
     L.nslots = capacity;
     return L;
@@ -841,19 +862,41 @@ int Batch::reset_lists()
 
 int Batch::run_chunk(bool timed)
 {
+    int rc;
+    bool sampling = false;
+    const TuneKey key{device, tune_bucket(2ll * nwork)};
+    if ((rc = use_tiling(tuner_pick(key, &sampling)))) return rc;
+    // a sample needs a chunk in which every running member steps `chunk`
+    // times (no member reaches its end or an event before the chunk's last
+    // step, none fails)
+    long long running = 0;
+    std::vector<long long> step0(capacity, -1);
+    for (int i = 0; i < capacity; i++)
+        if (members[i] && members[i]->hctl.status == kRunning) {
+            step0[i] = members[i]->hctl.step;
+            running++;
+        }
     if (timed) THY_CK(cudaEventRecord(ev0, st));
     THY_CK(cudaGraphLaunch(gexec, st));
     if (timed) THY_CK(cudaEventRecord(ev1, st));
     THY_CK(cudaMemcpyAsync(h_ctl, d_ctl, capacity * sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, st));
     THY_CK(cudaStreamSynchronize(st));
+    float ms = 0;
     if (timed) {
-        float ms = 0;
         THY_CK(cudaEventElapsedTime(&ms, ev0, ev1));
         device_ms += ms;
     }
     launches += (long long)kLaunchesPerStep * chunk;
+    bool full = running > 0 && nwork > 0;
     for (int i = 0; i < capacity; i++)
-        if (members[i]) members[i]->hctl = h_ctl[i];
+        if (members[i]) {
+            members[i]->hctl = h_ctl[i];
+            if (step0[i] >= 0 && (h_ctl[i].status == kFailed || h_ctl[i].step != step0[i] + chunk)) full = false;
+        }
+    if (timed && sampling && full) {
+        tuner_sample(key, tiling, (double)ms / ((double)chunk * 2.0 * nwork));
+        tune_samples++;
+    }
     return THY_OK;
 }
 
@@ -1061,6 +1104,8 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
                 stats->tiles = s.hctl.step * (long long)s.units();
                 stats->deep_tiles = (long long)s.hctl.units_deep;
                 stats->dry_tiles = (long long)s.hctl.units_dry;
+                stats->tiling = thy_tiling{b.tiling.deep1, b.tiling.deep2, b.tiling.general};
+                stats->tune_samples = b.tune_samples;
             }
         }
         {
@@ -1208,6 +1253,62 @@ extern "C" int thy_session_fetch(thy_session *S, float *max_height, float *eta, 
 }
 
 extern "C" double thy_session_time(const thy_session *S) { return S ? S->s.hctl.t * S->s.Ts : 0.0; }
+
+extern "C" int thy_session_tune(thy_session *S, long long max_steps, long long *steps_done)
+{
+    if (!S || max_steps < 0) return THY_ERR_INVALID;
+    long long done = 0;
+    int rc = THY_OK;
+    const TuneKey key{S->b.device, tune_bucket(2ll * S->b.nwork)};
+    while (done < max_steps && !tuner_decided(key, nullptr) && S->s.hctl.t < S->s.t_end) {
+        long long k = 0;
+        if ((rc = thy_session_steps(S, std::min<long long>(S->b.chunk, max_steps - done), nullptr, &k))) break;
+        if (k <= 0) break;
+        done += k;
+    }
+    if (steps_done) *steps_done = done;
+    return rc;
+}
+
+extern "C" int thy_session_tiling(const thy_session *S, thy_tiling *t)
+{
+    if (!S || !t) return THY_ERR_INVALID;
+    *t = thy_tiling{S->b.tiling.deep1, S->b.tiling.deep2, S->b.tiling.general};
+    return THY_OK;
+}
+
+static bool tiling_ok(const thy_tiling *t)
+{
+    return t->deep1 >= 0 && t->deep1 < kTilingVariants && t->deep2 >= 0 && t->deep2 < kTilingVariants &&
+           t->general >= 0 && t->general < kTilingVariants;
+}
+
+extern "C" int thy_tiling_force(const thy_tiling *t)
+{
+    if (!t) {
+        tuner_force(nullptr);
+        return THY_OK;
+    }
+    if (!tiling_ok(t)) return THY_ERR_INVALID;
+    Tiling x;
+    x.deep1 = t->deep1;
+    x.deep2 = t->deep2;
+    x.general = t->general;
+    tuner_force(&x);
+    return THY_OK;
+}
+
+extern "C" int thy_tiling_tuned(long long units, thy_tiling *best)
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+    Tiling t;
+    const bool done = tuner_decided(TuneKey{dev, tune_bucket(units)}, &t);
+    if (best) *best = thy_tiling{t.deep1, t.deep2, t.general};
+    return done ? 1 : 0;
+}
+
+extern "C" void thy_tuner_clear(void) { tuner_clear(); }
 
 extern "C" void thy_session_close(thy_session *S)
 {

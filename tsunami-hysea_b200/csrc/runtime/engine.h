@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <memory>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -88,7 +89,8 @@ struct DevScenario {
 };
 
 // A set of scenarios stepped together: one work list over all their tiles,
-// one CUDA graph of `chunk` steps (kLaunchesPerStep launches per step).
+// one CUDA graph of `chunk` steps (kLaunchesPerStep launches per step) per
+// warp tiling the autotuner has run it with (tuner.h).
 struct Batch {
     std::vector<DevScenario *> members;
     ScenarioDev *d_table = nullptr;
@@ -102,13 +104,15 @@ struct Batch {
     int capacity = 0;
     int work_capacity = 0;
     int nwork = 0;
-    int grid = 0;
-    int deep_grid[2] = {1, 1};
     int chunk = 16;
+    int device = 0;
+    Tiling tiling;                     // of gexec
+    std::vector<std::pair<Tiling, cudaGraphExec_t>> graphs;   // captured per tiling, current capacity
+    long long tune_samples = 0;        // chunks timed for the autotuner
     cudaStream_t st = nullptr;
     cudaStream_t st_side = nullptr;    // second branch of the captured graph (deep-water kernels)
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    cudaGraphExec_t gexec = nullptr;
+    cudaGraphExec_t gexec = nullptr;   // graph of the current tiling
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double device_ms = 0;
     long long launches = 0;
@@ -120,10 +124,14 @@ struct Batch {
     // upload the member table and the work list (of the members with
     // selected[slot] != 0, all of them without a selection) and classify
     int update(const std::vector<char> *selected = nullptr);
-    int capture();                    // (re)capture the step graph for the current capacity
+    int capture();                    // (re)capture the step graph of `tiling` for the current capacity
+    int use_tiling(const Tiling &t);  // switch graphs (capturing the tiling's graph if it has none)
+    void drop_graphs();
     int rebuild();                    // update(), and capture() when there is no graph yet
     int initial_dt_of(DevScenario *s);   // initial dt of one member (phase 0 over its units only)
-    int run_chunk(bool timed);       // one graph launch + control download (synchronous)
+    // one graph launch + control download (synchronous); the tiling is the
+    // autotuner's pick, and a full timed chunk is one of its samples
+    int run_chunk(bool timed);
     StepLaunch params() const;
     int reset_lists();               // classify again: after the host changed a member's state
 };

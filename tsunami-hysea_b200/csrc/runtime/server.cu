@@ -78,6 +78,8 @@ static void complete(thy_server *S, int slot, int status)
     st.tiles = s.hctl.step * s.units();
     st.deep_tiles = (long long)s.hctl.units_deep;
     st.dry_tiles = (long long)s.hctl.units_dry;
+    st.tiling = thy_tiling{S->b.tiling.deep1, S->b.tiling.deep2, S->b.tiling.general};
+    st.tune_samples = S->b.tune_samples;   // of the batch, so far
     if (status == THY_OK && a->r.o) {
         const auto t0 = Clock::now();
         status = s.finish(a->r.o, S->st);

@@ -1,0 +1,39 @@
+// Autotuner of the stepping kernels' warp tilings (kernels.h: Tiling).
+//
+// A tiling does not change any cell's arithmetic, only how the warps of a CTA
+// share a work unit and how many CTAs an SM keeps, so the tuner times real
+// chunks of real runs: every full chunk a batch steps is one sample of the
+// tiling it ran with (device time per work-list unit and step).  Samples are
+// kept per key = (device, work-list size bucket: ceil log2 of the units a step
+// visits), process-wide, so that every batch and every run of a size class
+// shares one search.  The search is coordinate descent over the three
+// kernels (deep phase 2, deep phase 1, general), each dimension timing the
+// incumbent and its two alternatives round robin, kRounds samples each, the
+// minimum of each kept; an alternative replaces the incumbent when it is more
+// than 1 % faster.  A decided key runs its best tiling from then on.
+//
+// Environment: THY_TILING="d1,d2,g" forces a tiling (variant indices);
+// THY_TUNE=0 keeps the default tiling; THY_TUNE_CACHE=<file> keeps decided
+// keys across processes (one line per key: device name, SM count, bucket,
+// tiling).
+#pragma once
+#include "../kernels/kernels.h"
+
+namespace thy {
+
+struct TuneKey {
+    int device;
+    int bucket;
+};
+
+int tune_bucket(long long units);                    // ceil log2 (>= 0)
+// tiling for the next chunk of a batch with this key; *sampling: the chunk's
+// time is wanted
+Tiling tuner_pick(const TuneKey &k, bool *sampling);
+// one sample: the tiling a full chunk ran with, device ms per unit-step
+void tuner_sample(const TuneKey &k, const Tiling &t, double ms_per_unit_step);
+bool tuner_decided(const TuneKey &k, Tiling *best);
+void tuner_force(const Tiling *t);                   // nullptr: tune again
+void tuner_clear();                                  // forget every key (not the cache file)
+
+}  // namespace thy

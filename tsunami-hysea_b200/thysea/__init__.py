@@ -205,8 +205,37 @@ def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = Tru
                loop_seconds=st.loop_seconds, device_ms=st.device_loop_ms, kernel_launches=st.kernel_launches,
                nsnaps=st.snapshots, nseries=st.series_samples, tiles=st.tiles, deep_tiles=st.deep_tiles,
                dry_tiles=st.dry_tiles, setup_seconds=st.setup_seconds, output_seconds=st.output_seconds,
-               total_seconds=st.total_seconds)
+               total_seconds=st.total_seconds, tiling=(st.tiling.deep1, st.tiling.deep2, st.tiling.general),
+               tune_samples=st.tune_samples)
     return res
+
+
+# Warp tilings of the stepping kernels (thy_tiling): row groups per work unit
+# of each variant index, per kernel.  Results never depend on the tiling.
+TILING_GROUPS = {"deep1": (3, 2, 4), "deep2": (2, 1, 3), "general": (2, 1, 4)}
+
+
+def force_tiling(tiling=None):
+    """Run every later chunk with tiling (deep1, deep2, general) variant
+    indices; None: autotune again (thy_tiling_force)."""
+    if tiling is None:
+        _check(_ffi.lib().thy_tiling_force(None), "thy_tiling_force")
+        return
+    t = _ffi.Tiling(*tiling)
+    _check(_ffi.lib().thy_tiling_force(ctypes.byref(t)), "thy_tiling_force")
+
+
+def tuned_tiling(units: int):
+    """(decided, (deep1, deep2, general)) of the autotuner for a work size of
+    `units` work units per step on the current device (thy_tiling_tuned)."""
+    t = _ffi.Tiling()
+    done = _ffi.lib().thy_tiling_tuned(units, ctypes.byref(t))
+    return bool(done), (t.deep1, t.deep2, t.general)
+
+
+def clear_tuner():
+    """Forget every tiling the autotuner decided in this process."""
+    _ffi.lib().thy_tuner_clear()
 
 
 class Session:
@@ -230,6 +259,19 @@ class Session:
 
     def time(self) -> float:
         return float(_ffi.lib().thy_session_time(self._h))
+
+    def tune(self, max_steps: int = 1 << 30) -> int:
+        """Steps (real steps of the run) until the autotuner has decided the
+        tiling for this problem's work size; returns the steps taken."""
+        k = ctypes.c_longlong()
+        _check(_ffi.lib().thy_session_tune(self._h, max_steps, ctypes.byref(k)), "thy_session_tune")
+        return k.value
+
+    def tiling(self):
+        """(deep1, deep2, general) variant indices of the last chunk"""
+        t = _ffi.Tiling()
+        _check(_ffi.lib().thy_session_tiling(self._h, ctypes.byref(t)), "thy_session_tiling")
+        return t.deep1, t.deep2, t.general
 
     def profile(self, k: int):
         """k individually launched steps; returns the average (phase-1 ms, phase-2 ms)."""
@@ -296,7 +338,8 @@ class Server:
                "done_at": time.perf_counter()}
         if stats_ptr:
             st = ctypes.cast(stats_ptr, ctypes.POINTER(_ffi.Stats)).contents
-            res["stats"] = {k: getattr(st, k) for k, _ in _ffi.Stats._fields_}
+            res["stats"] = {k: getattr(st, k) for k, _ in _ffi.Stats._fields_ if k != "tiling"}
+            res["stats"]["tiling"] = (st.tiling.deep1, st.tiling.deep2, st.tiling.general)
         self.results[int(request)] = res
 
     def submit(self, problem, out: Optional[Dict[str, np.ndarray]] = None) -> int:

@@ -62,6 +62,10 @@ class Outputs(ctypes.Structure):
     ]
 
 
+class Tiling(ctypes.Structure):
+    _fields_ = [("deep1", ctypes.c_int), ("deep2", ctypes.c_int), ("general", ctypes.c_int)]
+
+
 class Stats(ctypes.Structure):
     _fields_ = [
         ("steps", ctypes.c_longlong), ("final_time_s", ctypes.c_double), ("first_dt_s", ctypes.c_double),
@@ -69,6 +73,7 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_longlong), ("snapshots", ctypes.c_int), ("series_samples", ctypes.c_int),
         ("tiles", ctypes.c_longlong), ("deep_tiles", ctypes.c_longlong), ("dry_tiles", ctypes.c_longlong),
         ("setup_seconds", ctypes.c_double), ("output_seconds", ctypes.c_double), ("total_seconds", ctypes.c_double),
+        ("tiling", Tiling), ("tune_samples", ctypes.c_longlong),
     ]
 
 
@@ -126,6 +131,11 @@ SIGNATURES = {
     "thy_session_tiles": ([ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong),
                            ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "thy_session_close": ([ctypes.c_void_p], None),
+    "thy_session_tune": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "thy_session_tiling": ([ctypes.c_void_p, ctypes.POINTER(Tiling)], ctypes.c_int),
+    "thy_tiling_force": ([ctypes.POINTER(Tiling)], ctypes.c_int),
+    "thy_tiling_tuned": ([ctypes.c_longlong, ctypes.POINTER(Tiling)], ctypes.c_int),
+    "thy_tuner_clear": ([], None),
     "thy_server_open": ([ctypes.POINTER(ServerOpts), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "thy_server_submit": ([ctypes.c_void_p, ctypes.POINTER(ProblemC), ctypes.POINTER(Outputs), DoneFn,
                            ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
