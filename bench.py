@@ -3,7 +3,7 @@
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
-Workload (BASELINE config 2): one 4096 x 4096 scenario, Gaussian-random-field
+Workload: one 4096 x 4096 scenario, Gaussian-random-field
 bathymetry with a shelf and ~10 % dry cells, four contiguous Okada
 subfaults, 3600 s simulated; seeded synthetic inputs (no dataset exists).
 
@@ -307,7 +307,7 @@ def run_ours(a, dist: Dist):
         "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": dist.world, "steps": a.steps,
         "warmup": a.warmup, "ms_per_step": round(dev_s * 1e3 / a.steps, 5), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": {"workload": f"single_large {p.nx}x{p.ny} cells, 4 Okada subfaults, 3600 s simulated (BASELINE config 2)",
+        "config": {"workload": f"single_large {p.nx}x{p.ny} cells, 4 Okada subfaults, 3600 s simulated",
                    "cells": cells, "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
                    "l2": "state 268 MB > 126 MB L2, no flush", "simulated_s_per_step": None,
                    "tiling": {k: thysea.TILING_GROUPS[k][v] for k, v in zip(("deep1", "deep2", "general"), tiling)},
@@ -345,7 +345,7 @@ def run_reference(a, dist: Dist):
         "impl": "reference", "metric": METRIC, "value": round(value, 1), "unit": METRIC, "n_gpus": dist.world,
         "steps": k, "warmup": a.warmup, "ms_per_step": round(sec * 1e3 / k, 4), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded)",
-        "config": {"workload": f"single_large {p.nx}x{p.ny} cells, 4 Okada subfaults, 3600 s simulated (BASELINE config 2)",
+        "config": {"workload": f"single_large {p.nx}x{p.ny} cells, 4 Okada subfaults, 3600 s simulated",
                    "sample": sample},
         "cpu_baseline": {"value": round(value, 1), "unit": METRIC, "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": round(value, 1), "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -387,7 +387,9 @@ def _fifo(arrivals, service):
 
 
 def run_batched(a, dist):
-    """BASELINE configs 3-5 through the multi-scenario runtime (thy_server),
+    """The many-scenario workloads (batch: 64 scenarios of 2048^2 on one
+    bathymetry; mixed: 32 scenarios of sides 256-4096; serving: a Poisson
+    request stream) through the multi-scenario runtime (thy_server),
     next to the plain path (one thy_run per scenario) on the same inputs.
 
       batch:   64 scenarios on one shared 2048^2 bathymetry, one seeded
@@ -542,6 +544,43 @@ def run_batched(a, dist):
     }
 
 
+def run_tilings(a, dist):
+    """Per-tiling device times of the single-scenario workload (side --n):
+    one session; for every tiling that differs from the default in one kernel,
+    16 individually launched steps (per-launch ms) and 64 graph-launched steps
+    (ms per step), then the autotuner's own pick from a fresh search.  Not the
+    headline line: it shows what the autotuner chooses between."""
+    import thysea
+    from thysea import synth
+
+    if thysea.device_count() == 0:
+        raise SystemExit("bench: no CUDA device")
+    thysea._ffi.lib().thy_set_device(dist.local)
+    p = synth.single_large(n=a.n, sim_time=3600.0)
+    sess = thysea.Session(thysea.Prepared(p))
+    sess.steps(a.warmup)
+    names = ("deep_phase1", "general_phase1", "classify", "deep_phase2", "general_phase2", "controller")
+    rows = []
+    try:
+        for t in [(0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (0, 2, 0), (0, 0, 1), (0, 0, 2)]:
+            thysea.force_tiling(t)
+            sess.steps(32)
+            ms6 = sess.profile_launches(16)
+            dms, k = sess.steps(64)
+            groups = {n: thysea.TILING_GROUPS[n][v] for n, v in zip(("deep1", "deep2", "general"), t)}
+            rows.append({"tiling": t, "row_groups": groups, "ms_per_step": round(dms / max(k, 1), 5),
+                         "launch_ms": {n: round(v, 5) for n, v in zip(names, ms6)}})
+    finally:
+        thysea.force_tiling(None)
+    thysea.clear_tuner()
+    steps = sess.tune()
+    pick = sess.tiling()
+    sess.close()
+    return {"metric": "ms per step by warp tiling", "unit": "ms", "n_gpus": 1, "workload": "tilings",
+            "config": {"workload": f"single_large {p.nx}x{p.ny}", "warmup": a.warmup}, "tilings": rows,
+            "autotuner": {"pick": pick, "tune_steps": steps}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -554,8 +593,10 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=400)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["single", "batch", "mixed", "serving"], default="single",
-                    help="single: config 2 (the headline line); batch / mixed / serving: configs 3 / 4 / 5")
+    ap.add_argument("--workload", choices=["single", "batch", "mixed", "serving", "tilings"], default="single",
+                    help="single: one 4096^2 scenario (the headline line); batch: 64 x 2048^2 on one "
+                         "bathymetry; mixed: 32 scenarios of sides 256-4096; serving: Poisson requests; "
+                         "tilings: device time of each warp tiling (side --n)")
     ap.add_argument("--count", type=int, default=0, help="batch / mixed: number of scenarios (0: 64 / 32)")
     ap.add_argument("--rate", type=float, default=2.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
@@ -566,6 +607,8 @@ def main():
     try:
         if a.impl == "reference":
             line = run_reference(a, dist)
+        elif a.workload == "tilings":
+            line = run_tilings(a, dist) if dist.rank == 0 else None
         elif a.workload != "single":
             line = run_batched(a, dist)
         else:

@@ -32,7 +32,7 @@ def _assert_parity(c, snaps=True):
 
 
 def test_plain_small_quarter(gpu):
-    """config 1 shape at 256^2: open borders, one fault, 600 s, 16 gauges"""
+    """the plain small problem's shape at 256^2: open borders, one fault, 600 s, 16 gauges"""
     p = synth.plain_small(nx=256, ny=256, sim_time=600.0, save_time=200.0, series_time=60.0, npoints=16)
     g, r, c = _both(gpu, p)
     _assert_parity(c)

@@ -146,7 +146,7 @@ def shelf_bathymetry(nx: int, ny: int, rng: np.random.Generator, dry_fraction: f
 
 
 # ---------------------------------------------------------------------------
-# the BASELINE configurations
+# the benchmark workloads
 # ---------------------------------------------------------------------------
 
 def seeded_points(lon, lat, z, n: int, rng: np.random.Generator) -> np.ndarray:
@@ -158,7 +158,7 @@ def seeded_points(lon, lat, z, n: int, rng: np.random.Generator) -> np.ndarray:
 
 def plain_small(nx: int = 512, ny: int = 512, seed: int = 1, sim_time: float = 600.0,
                 save_time: float = 300.0, series_time: float = 60.0, npoints: int = 16) -> Problem:
-    """Config 1: linear eastern shelf to +200 m land, -4000 m ocean, sigma 20 m
+    """Plain small problem: linear eastern shelf to +200 m land, -4000 m ocean, sigma 20 m
     noise, one Okada fault (100 x 50 km, 5 m slip, strike 0, dip 15, rake 90,
     top 10 km) centred at 30 % of the width."""
     rng = np.random.default_rng(seed)
@@ -178,7 +178,7 @@ def plain_small(nx: int = 512, ny: int = 512, seed: int = 1, sim_time: float = 6
 
 def single_large(n: int = 4096, seed: int = 2, sim_time: float = 3600.0, save_time: float = -1.0,
                  npoints: int = 0) -> Problem:
-    """Config 2: random-field bathymetry with shelf and ~10 % dry cells; four
+    """Single large scenario: random-field bathymetry with shelf and ~10 % dry cells; four
     contiguous 100 x 50 km subfaults along strike 0 (dip 15, rake 90, top
     10 km), slip U(2, 8) m."""
     rng = np.random.default_rng(seed)
@@ -211,7 +211,7 @@ def random_fault(lon, lat, z, rng: np.random.Generator, time: float = 0.0) -> Fa
 
 
 def batch_uniform(count: int = 64, n: int = 2048, seed: int = 3, sim_time: float = 1800.0) -> List[Problem]:
-    """Config 3: ``count`` scenarios on one shared random-field bathymetry."""
+    """Uniform batch: ``count`` scenarios on one shared random-field bathymetry."""
     rng = np.random.default_rng(seed)
     lon, lat = lonlat_grid(n, n)
     z = shelf_bathymetry(n, n, rng)
@@ -231,13 +231,13 @@ def mixed_scenario(rng: np.random.Generator, name: str, side_range=(256, 4096), 
 
 
 def mixed(count: int = 32, seed: int = 4, side_range=(256, 4096), time_range=(600.0, 7200.0)) -> List[Problem]:
-    """Config 4: log-uniform sides, own bathymetry, one fault, U(600, 7200) s."""
+    """Mixed-size batch: log-uniform sides, own bathymetry, one fault, U(600, 7200) s."""
     rng = np.random.default_rng(seed)
     return [mixed_scenario(rng, f"mixed_{k:03d}", side_range, time_range) for k in range(count)]
 
 
 def poisson_arrivals(rate: float = 2.0, duration: float = 600.0, seed: int = 5) -> np.ndarray:
-    """Config 5: arrival times (s) of a Poisson stream."""
+    """Serving stream: arrival times (s) of a Poisson stream."""
     rng = np.random.default_rng(seed)
     t, out = 0.0, []
     while True:
