@@ -215,13 +215,18 @@ def run_ours(a, dist: Dist):
     p = synth.single_large(n=a.n, sim_time=3600.0)
     prep = thysea.Prepared(p)
     cells = p.nx * p.ny
+    # one full untimed run first: its chunks are the autotuner's samples for
+    # every work mix the run passes through (keys of deep and general units
+    # per step), so that the timed steps and the end-to-end runs below use
+    # decided tilings (with THY_TILING or THY_TUNE=0 set the tuner is off)
+    tuning_run = None
+    if not os.environ.get("THY_TILING") and os.environ.get("THY_TUNE", "1") != "0":
+        r = thysea.run(prep, snapshots=False, series=False)
+        tuning_run = {"steps": int(r["iterations"]), "tune_samples": int(r["tune_samples"])}
     sess = thysea.Session(prep)
-    # the autotuner times its candidate tilings on the first chunks (real
-    # steps of this run) before the clock starts; the timed steps and the
-    # end-to-end runs use its pick
     tune_steps = sess.tune()
-    tiling = sess.tiling()
     sess.steps(a.warmup)
+    tiling = sess.tiling()
     l0 = sess.launches()
     clk = ClockSampler(dist.local)
     clk.start()
@@ -311,7 +316,8 @@ def run_ours(a, dist: Dist):
                    "cells": cells, "parallelism": f"replicas x{dist.world}" if dist.world > 1 else "single GPU",
                    "l2": "state 268 MB > 126 MB L2, no flush", "simulated_s_per_step": None,
                    "tiling": {k: thysea.TILING_GROUPS[k][v] for k, v in zip(("deep1", "deep2", "general"), tiling)},
-                   "tiling_note": "row groups per work unit picked by the autotuner", "tune_steps": int(tune_steps)},
+                   "tiling_note": "row groups per work unit at the start of the timed steps, picked by the autotuner",
+                   "tuning_run": tuning_run, "tune_steps": int(tune_steps)},
         "roofline": roofline, "e2e": e2e, "cpu_baseline": cpu, "clocks": clocks, "gpu_launches": int(launches),
         "wall_s_timed": round(wall, 4),
     }
@@ -545,11 +551,13 @@ def run_batched(a, dist):
 
 
 def run_tilings(a, dist):
-    """Per-tiling device times of the single-scenario workload (side --n):
-    one session; for every tiling that differs from the default in one kernel,
-    16 individually launched steps (per-launch ms) and 64 graph-launched steps
-    (ms per step), then the autotuner's own pick from a fresh search.  Not the
-    headline line: it shows what the autotuner chooses between."""
+    """Per-tiling device times of the single-scenario workload (side --n), at
+    one stage of the run: the autotuner first decides from a fresh search
+    (real steps), then every tiling that differs from the default in one
+    kernel, and the tuner's pick, run one 16-step chunk each, round robin for
+    --tiling-rounds rounds (so that all see the same work mix), with two
+    individually launched steps each per round for the per-launch times.
+    Not the headline line: it shows what the autotuner chooses between."""
     import thysea
     from thysea import synth
 
@@ -559,26 +567,40 @@ def run_tilings(a, dist):
     p = synth.single_large(n=a.n, sim_time=3600.0)
     sess = thysea.Session(thysea.Prepared(p))
     sess.steps(a.warmup)
+    thysea.force_tiling(None)
+    thysea.clear_tuner()
+    t0 = sess.time()
+    tune_steps = sess.tune()
+    decided, pick = sess.tuned()
     names = ("deep_phase1", "general_phase1", "classify", "deep_phase2", "general_phase2", "controller")
-    rows = []
+    tilings = [(0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (0, 2, 0), (0, 0, 1), (0, 0, 2)]
+    if tuple(pick) not in tilings:
+        tilings.append(tuple(pick))
+    chunk = {t: [] for t in tilings}
+    launch = {t: [] for t in tilings}
+    t1 = sess.time()
     try:
-        for t in [(0, 0, 0), (1, 0, 0), (2, 0, 0), (0, 1, 0), (0, 2, 0), (0, 0, 1), (0, 0, 2)]:
-            thysea.force_tiling(t)
-            sess.steps(32)
-            ms6 = sess.profile_launches(16)
-            dms, k = sess.steps(64)
-            groups = {n: thysea.TILING_GROUPS[n][v] for n, v in zip(("deep1", "deep2", "general"), t)}
-            rows.append({"tiling": t, "row_groups": groups, "ms_per_step": round(dms / max(k, 1), 5),
-                         "launch_ms": {n: round(v, 5) for n, v in zip(names, ms6)}})
+        for _ in range(a.tiling_rounds):
+            for t in tilings:
+                thysea.force_tiling(t)
+                dms, k = sess.steps(16)
+                chunk[t].append(dms / max(k, 1))
+                launch[t].append(sess.profile_launches(2))
     finally:
         thysea.force_tiling(None)
-    thysea.clear_tuner()
-    steps = sess.tune()
-    pick = sess.tiling()
+    t2 = sess.time()
     sess.close()
+    rows = []
+    for t in tilings:
+        groups = {n: thysea.TILING_GROUPS[n][v] for n, v in zip(("deep1", "deep2", "general"), t)}
+        per = [statistics.mean(x[i] for x in launch[t]) for i in range(6)]
+        rows.append({"tiling": t, "row_groups": groups, "ms_per_step_min": round(min(chunk[t]), 5),
+                     "ms_per_step_median": round(statistics.median(chunk[t]), 5),
+                     "launch_ms": {n: round(v, 5) for n, v in zip(names, per)}})
     return {"metric": "ms per step by warp tiling", "unit": "ms", "n_gpus": 1, "workload": "tilings",
-            "config": {"workload": f"single_large {p.nx}x{p.ny}", "warmup": a.warmup}, "tilings": rows,
-            "autotuner": {"pick": pick, "tune_steps": steps}}
+            "config": {"workload": f"single_large {p.nx}x{p.ny}", "warmup": a.warmup, "rounds": a.tiling_rounds,
+                       "simulated_s": [round(t0, 1), round(t1, 1), round(t2, 1)]},
+            "tilings": rows, "autotuner": {"pick": list(pick), "decided": decided, "tune_steps": tune_steps}}
 
 
 def main():
@@ -601,6 +623,7 @@ def main():
     ap.add_argument("--rate", type=float, default=2.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="batch / mixed / serving: HBM budget")
+    ap.add_argument("--tiling-rounds", type=int, default=4, help="tilings: round-robin rounds")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     dist = Dist()

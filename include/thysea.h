@@ -224,18 +224,23 @@ double thy_session_time(const thy_session *s);    /* simulated time (s) */
    for this problem's work size, at most max_steps; *steps_done: steps taken */
 int thy_session_tune(thy_session *s, long long max_steps, long long *steps_done);
 int thy_session_tiling(const thy_session *s, thy_tiling *t);   /* tiling of the last chunk */
+/* 1 when the tiling for the session's current work (its last chunk's deep
+   and general units per step) is decided (*best set), 0 while tuning */
+int thy_session_tuned(const thy_session *s, thy_tiling *best);
 void thy_session_close(thy_session *s);
 
 /* Autotuner of the warp tilings.  Every full chunk of a run (of any entry
    point) is timed as one sample of the tiling it ran with; the search, per
-   device and work size (ceil log2 of the work units a step visits), is
-   coordinate descent over deep phase 2, deep phase 1 and the general kernel.
+   device and work of a step (ceil log2 of its deep units and of its general
+   units, estimated from each scenario's previous chunk), is coordinate
+   descent over deep phase 2, deep phase 1 and the general kernel.
    Environment: THY_TILING="d1,d2,g" forces a tiling, THY_TUNE=0 keeps the
    default, THY_TUNE_CACHE=<file> keeps decided tilings across processes. */
 int thy_tiling_force(const thy_tiling *t);          /* NULL: autotune again */
-/* 1 when the tiling for `units` work units per step is decided on the current
-   device (*best set), 0 while tuning (*best: the incumbent) */
-int thy_tiling_tuned(long long units, thy_tiling *best);
+/* 1 when the tiling for steps of deep_units deep and general_units general
+   work units is decided on the current device (*best set), 0 while tuning
+   (*best: the incumbent) */
+int thy_tiling_tuned(double deep_units, double general_units, thy_tiling *best);
 void thy_tuner_clear(void);                         /* forget every decision of this process */
 
 /* Multi-scenario runtime (batched and serving use): scenarios submitted at

@@ -52,7 +52,7 @@ int main(int argc, char **argv)
 {
     if (argc < 2) return 2;
     const char *sc = argv[1];
-    const TuneKey k{0, 20};
+    const TuneKey k{0, 13, 10};
     int chunks = 0;
     if (!std::strcmp(sc, "descent")) {
         // deep phase 2 best at variant 1, deep phase 1 at 2, general at 0
@@ -84,7 +84,7 @@ int main(int argc, char **argv)
     } else if (!std::strcmp(sc, "keys")) {
         Costs a{{1.0, 0.5, 1.0}, {1.0, 1.0, 1.0}, {1.0, 1.0, 1.0}};
         Costs b{{1.0, 1.0, 1.0}, {1.0, 1.0, 1.0}, {1.0, 1.0, 0.5}};
-        const TuneKey k2{0, 7};
+        const TuneKey k2{0, 7, 3};
         run_to_decision(k, a, 0.0, &chunks);
         print("keys-a", k, chunks);
         run_to_decision(k2, b, 0.0, &chunks);

@@ -85,7 +85,7 @@ def test_cache_file_round_trip(driver, tmp_path):
     # read back after the in-process state is cleared: decided without samples
     assert _field(out[1], "done") == "1" and _field(out[1], "tiling") == "1,2,0"
     lines = open(path).read().split("\n")
-    assert lines[0].split()[2:] == ["20", "1", "2", "0"]
+    assert lines[0].split()[2:] == ["13", "10", "1", "2", "0"]   # deep and general buckets, tiling
     # a second process starts decided from the file
     out = _run(driver, "cache", {"THY_TUNE_CACHE": path})
     assert _field(out[0], "chunks") == "0" and _field(out[0], "tiling") == "1,2,0"
@@ -99,4 +99,5 @@ def test_abi_checks_tiling_arguments():
     assert L.thy_tiling_force(None) == 0
     assert L.thy_session_tune(None, 10, None) == thysea.THY_ERR_INVALID
     assert L.thy_session_tiling(None, None) == thysea.THY_ERR_INVALID
+    assert L.thy_session_tuned(None, None) == thysea.THY_ERR_INVALID
     assert set(thysea.TILING_GROUPS) == {"deep1", "deep2", "general"}

@@ -860,20 +860,38 @@ int Batch::reset_lists()
     return THY_OK;
 }
 
+TuneKey Batch::tune_key(bool *known, bool all_members) const
+{
+    double deep = 0, general = 0;
+    bool all = true;
+    for (auto *m : members)
+        if (m && (all_members || m->hctl.status == kRunning)) {
+            deep += m->mix_deep;
+            general += std::max(0.0, (double)m->units() - m->mix_deep - m->mix_dry);
+            all = all && m->mix_known;
+        }
+    if (known) *known = all;
+    return TuneKey{device, tune_bucket(deep), tune_bucket(general)};
+}
+
 int Batch::run_chunk(bool timed)
 {
     int rc;
-    bool sampling = false;
-    const TuneKey key{device, tune_bucket(2ll * nwork)};
+    bool sampling = false, known = false;
+    const TuneKey key = tune_key(&known);
     if ((rc = use_tiling(tuner_pick(key, &sampling)))) return rc;
     // a sample needs a chunk in which every running member steps `chunk`
     // times (no member reaches its end or an event before the chunk's last
-    // step, none fails)
+    // step, none fails) and whose work mix was known beforehand
+    struct Before {
+        long long step;
+        unsigned long long deep, dry;
+    };
+    std::vector<Before> b0(capacity, Before{-1, 0, 0});
     long long running = 0;
-    std::vector<long long> step0(capacity, -1);
     for (int i = 0; i < capacity; i++)
         if (members[i] && members[i]->hctl.status == kRunning) {
-            step0[i] = members[i]->hctl.step;
+            b0[i] = Before{members[i]->hctl.step, members[i]->hctl.units_deep, members[i]->hctl.units_dry};
             running++;
         }
     if (timed) THY_CK(cudaEventRecord(ev0, st));
@@ -887,14 +905,26 @@ int Batch::run_chunk(bool timed)
         device_ms += ms;
     }
     launches += (long long)kLaunchesPerStep * chunk;
-    bool full = running > 0 && nwork > 0;
-    for (int i = 0; i < capacity; i++)
-        if (members[i]) {
-            members[i]->hctl = h_ctl[i];
-            if (step0[i] >= 0 && (h_ctl[i].status == kFailed || h_ctl[i].step != step0[i] + chunk)) full = false;
+    bool full = running > 0;
+    double stepped = 0;   // deep + general units stepped in the chunk
+    for (int i = 0; i < capacity; i++) {
+        DevScenario *m = members[i];
+        if (!m) continue;
+        m->hctl = h_ctl[i];
+        if (b0[i].step < 0) continue;
+        const long long k = m->hctl.step - b0[i].step;
+        if (m->hctl.status == kFailed || k != chunk) full = false;
+        if (k > 0) {
+            const double deep = (double)(m->hctl.units_deep - b0[i].deep);
+            const double dry = (double)(m->hctl.units_dry - b0[i].dry);
+            m->mix_deep = deep / k;
+            m->mix_dry = dry / k;
+            m->mix_known = true;
+            stepped += std::max(0.0, (double)m->units() * k - dry);
         }
-    if (timed && sampling && full) {
-        tuner_sample(key, tiling, (double)ms / ((double)chunk * 2.0 * nwork));
+    }
+    if (timed && sampling && full && known && stepped > 0) {
+        tuner_sample(key, tiling, (double)ms / stepped);
         tune_samples++;
     }
     return THY_OK;
@@ -1259,8 +1289,12 @@ extern "C" int thy_session_tune(thy_session *S, long long max_steps, long long *
     if (!S || max_steps < 0) return THY_ERR_INVALID;
     long long done = 0;
     int rc = THY_OK;
-    const TuneKey key{S->b.device, tune_bucket(2ll * S->b.nwork)};
-    while (done < max_steps && !tuner_decided(key, nullptr) && S->s.hctl.t < S->s.t_end) {
+    while (done < max_steps && S->s.hctl.t < S->s.t_end) {
+        // the session's scenario waits between calls (its status is not
+        // running): its key counts it all the same
+        bool known = false;
+        const TuneKey key = S->b.tune_key(&known, true);
+        if (known && tuner_decided(key, nullptr)) break;
         long long k = 0;
         if ((rc = thy_session_steps(S, std::min<long long>(S->b.chunk, max_steps - done), nullptr, &k))) break;
         if (k <= 0) break;
@@ -1275,6 +1309,17 @@ extern "C" int thy_session_tiling(const thy_session *S, thy_tiling *t)
     if (!S || !t) return THY_ERR_INVALID;
     *t = thy_tiling{S->b.tiling.deep1, S->b.tiling.deep2, S->b.tiling.general};
     return THY_OK;
+}
+
+extern "C" int thy_session_tuned(const thy_session *S, thy_tiling *best)
+{
+    if (!S) return THY_ERR_INVALID;
+    bool known = false;
+    const TuneKey key = S->b.tune_key(&known, true);
+    Tiling t;
+    const bool done = tuner_decided(key, &t);
+    if (best) *best = thy_tiling{t.deep1, t.deep2, t.general};
+    return (known && done) ? 1 : 0;
 }
 
 static bool tiling_ok(const thy_tiling *t)
@@ -1298,12 +1343,12 @@ extern "C" int thy_tiling_force(const thy_tiling *t)
     return THY_OK;
 }
 
-extern "C" int thy_tiling_tuned(long long units, thy_tiling *best)
+extern "C" int thy_tiling_tuned(double deep_units, double general_units, thy_tiling *best)
 {
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
     Tiling t;
-    const bool done = tuner_decided(TuneKey{dev, tune_bucket(units)}, &t);
+    const bool done = tuner_decided(TuneKey{dev, tune_bucket(deep_units), tune_bucket(general_units)}, &t);
     if (best) *best = thy_tiling{t.deep1, t.deep2, t.general};
     return done ? 1 : 0;
 }

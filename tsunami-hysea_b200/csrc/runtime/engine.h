@@ -14,6 +14,7 @@
 #include "../../../include/thysea.h"
 #include "../kernels/device.cuh"
 #include "../kernels/kernels.h"
+#include "tuner.h"
 
 namespace thy {
 
@@ -70,6 +71,10 @@ struct DevScenario {
     int snapshots = 0, series = 0;
     std::vector<float> ts_min, ts_max;
     double first_dt_s = 0;
+    // work mix of the last chunk it stepped (per step): deep units, skipped
+    // dry units; the autotuner's key for the chunks that follow
+    double mix_deep = 0, mix_dry = 0;
+    bool mix_known = false;
     std::unique_ptr<OutputPipe> pipe;   // created at the first snapshot / gauge sample
 
     long long units() const { return (long long)desc.tiles_x * ((ny + kHalfRows - 1) / kHalfRows); }   // work units
@@ -132,6 +137,11 @@ struct Batch {
     // one graph launch + control download (synchronous); the tiling is the
     // autotuner's pick, and a full timed chunk is one of its samples
     int run_chunk(bool timed);
+    // the autotuner's key of the next chunk: this device, the deep and
+    // general units per step estimated from each stepping member's last
+    // chunk (members with status running; every member when all_members);
+    // *known: each of them has been measured
+    TuneKey tune_key(bool *known = nullptr, bool all_members = false) const;
     StepLaunch params() const;
     int reset_lists();               // classify again: after the host changed a member's state
 };

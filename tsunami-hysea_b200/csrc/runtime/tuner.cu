@@ -10,6 +10,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <tuple>
 #include <utility>
 
 namespace thy {
@@ -46,7 +47,7 @@ Tiling candidate(const Entry &e, int j)
 
 struct State {
     std::mutex mu;
-    std::map<std::pair<int, int>, Entry> keys;
+    std::map<std::tuple<int, int, int>, Entry> keys;
     bool env_read = false;
     bool forced = false;
     bool off = false;
@@ -106,11 +107,11 @@ void load_cache(State &s, int device)
     if (!f) return;
     const std::string id = device_id(device);
     char name[256];
-    int sms, bucket, a, b, c;
-    while (std::fscanf(f, "%255s %d %d %d %d %d", name, &sms, &bucket, &a, &b, &c) == 6) {
+    int sms, bd, bg, a, b, c;
+    while (std::fscanf(f, "%255s %d %d %d %d %d %d", name, &sms, &bd, &bg, &a, &b, &c) == 7) {
         if (std::string(name) + " " + std::to_string(sms) != id) continue;
         if (a < 0 || b < 0 || c < 0 || a >= kTilingVariants || b >= kTilingVariants || c >= kTilingVariants) continue;
-        Entry &e = s.keys[{device, bucket}];
+        Entry &e = s.keys[std::make_tuple(device, bd, bg)];
         e.inc.deep1 = a;
         e.inc.deep2 = b;
         e.inc.general = c;
@@ -119,12 +120,12 @@ void load_cache(State &s, int device)
     std::fclose(f);
 }
 
-void store_cache(const State &s, int device, int bucket, const Tiling &t)
+void store_cache(const State &s, const TuneKey &k, const Tiling &t)
 {
     if (s.cache_path.empty()) return;
     FILE *f = std::fopen(s.cache_path.c_str(), "a");
     if (!f) return;
-    std::fprintf(f, "%s %d %d %d %d\n", device_id(device).c_str(), bucket, t.deep1, t.deep2, t.general);
+    std::fprintf(f, "%s %d %d %d %d %d\n", device_id(k.device).c_str(), k.deep, k.general, t.deep1, t.deep2, t.general);
     std::fclose(f);
 }
 
@@ -132,15 +133,15 @@ Entry &entry(State &s, const TuneKey &k)
 {
     read_env(s);
     load_cache(s, k.device);
-    return s.keys[{k.device, k.bucket}];
+    return s.keys[std::make_tuple(k.device, k.deep, k.general)];
 }
 
 }  // namespace
 
-int tune_bucket(long long units)
+int tune_bucket(double units)
 {
     int b = 0;
-    while (b < 62 && (1ll << b) < units) b++;
+    while (b < 62 && (double)(1ll << b) < units) b++;
     return b;
 }
 
@@ -175,7 +176,7 @@ void tuner_sample(const TuneKey &k, const Tiling &t, double v)
     for (double &b : e.best) b = 1e300;
     if (++e.dim == kDims) {
         e.done = true;
-        store_cache(s, k.device, k.bucket, e.inc);
+        store_cache(s, k, e.inc);
     }
 }
 

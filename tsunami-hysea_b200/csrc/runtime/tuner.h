@@ -3,9 +3,8 @@
 // A tiling does not change any cell's arithmetic, only how the warps of a CTA
 // share a work unit and how many CTAs an SM keeps, so the tuner times real
 // chunks of real runs: every full chunk a batch steps is one sample of the
-// tiling it ran with (device time per work-list unit and step).  Samples are
-// kept per key = (device, work-list size bucket: ceil log2 of the units a step
-// visits), process-wide, so that every batch and every run of a size class
+// tiling it ran with (device time per stepped unit).  Samples are kept per key
+// (below), process-wide, so that every batch and every run with that work
 // shares one search.  The search is coordinate descent over the three
 // kernels (deep phase 2, deep phase 1, general), each dimension timing the
 // incumbent and its two alternatives round robin, kRounds samples each, the
@@ -14,23 +13,27 @@
 //
 // Environment: THY_TILING="d1,d2,g" forces a tiling (variant indices);
 // THY_TUNE=0 keeps the default tiling; THY_TUNE_CACHE=<file> keeps decided
-// keys across processes (one line per key: device name, SM count, bucket,
-// tiling).
+// keys across processes (one line per key: device name, SM count, deep and
+// general buckets, tiling).
 #pragma once
 #include "../kernels/kernels.h"
 
 namespace thy {
 
+// Key: the device and the work of a step, as ceil log2 buckets of its deep
+// units and of its general units (the best tiling of each kernel depends on
+// how many units it has to spread over the SMs).
 struct TuneKey {
     int device;
-    int bucket;
+    int deep;      // tune_bucket(deep units per step)
+    int general;   // tune_bucket(general units per step)
 };
 
-int tune_bucket(long long units);                    // ceil log2 (>= 0)
+int tune_bucket(double units);                       // ceil log2, 0 for units <= 1
 // tiling for the next chunk of a batch with this key; *sampling: the chunk's
 // time is wanted
 Tiling tuner_pick(const TuneKey &k, bool *sampling);
-// one sample: the tiling a full chunk ran with, device ms per unit-step
+// one sample: the tiling a full chunk ran with, device ms per stepped unit
 void tuner_sample(const TuneKey &k, const Tiling &t, double ms_per_unit_step);
 bool tuner_decided(const TuneKey &k, Tiling *best);
 void tuner_force(const Tiling *t);                   // nullptr: tune again

@@ -225,11 +225,12 @@ def force_tiling(tiling=None):
     _check(_ffi.lib().thy_tiling_force(ctypes.byref(t)), "thy_tiling_force")
 
 
-def tuned_tiling(units: int):
-    """(decided, (deep1, deep2, general)) of the autotuner for a work size of
-    `units` work units per step on the current device (thy_tiling_tuned)."""
+def tuned_tiling(deep_units: float, general_units: float):
+    """(decided, (deep1, deep2, general)) of the autotuner for steps of
+    deep_units deep and general_units general work units on the current
+    device (thy_tiling_tuned)."""
     t = _ffi.Tiling()
-    done = _ffi.lib().thy_tiling_tuned(units, ctypes.byref(t))
+    done = _ffi.lib().thy_tiling_tuned(float(deep_units), float(general_units), ctypes.byref(t))
     return bool(done), (t.deep1, t.deep2, t.general)
 
 
@@ -266,6 +267,12 @@ class Session:
         k = ctypes.c_longlong()
         _check(_ffi.lib().thy_session_tune(self._h, max_steps, ctypes.byref(k)), "thy_session_tune")
         return k.value
+
+    def tuned(self):
+        """(decided, (deep1, deep2, general)) for the session's current work"""
+        t = _ffi.Tiling()
+        done = _ffi.lib().thy_session_tuned(self._h, ctypes.byref(t))
+        return bool(done == 1), (t.deep1, t.deep2, t.general)
 
     def tiling(self):
         """(deep1, deep2, general) variant indices of the last chunk"""

@@ -134,7 +134,8 @@ SIGNATURES = {
     "thy_session_tune": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "thy_session_tiling": ([ctypes.c_void_p, ctypes.POINTER(Tiling)], ctypes.c_int),
     "thy_tiling_force": ([ctypes.POINTER(Tiling)], ctypes.c_int),
-    "thy_tiling_tuned": ([ctypes.c_longlong, ctypes.POINTER(Tiling)], ctypes.c_int),
+    "thy_tiling_tuned": ([ctypes.c_double, ctypes.c_double, ctypes.POINTER(Tiling)], ctypes.c_int),
+    "thy_session_tuned": ([ctypes.c_void_p, ctypes.POINTER(Tiling)], ctypes.c_int),
     "thy_tuner_clear": ([], None),
     "thy_server_open": ([ctypes.POINTER(ServerOpts), ctypes.POINTER(ctypes.c_void_p)], ctypes.c_int),
     "thy_server_submit": ([ctypes.c_void_p, ctypes.POINTER(ProblemC), ctypes.POINTER(Outputs), DoneFn,
