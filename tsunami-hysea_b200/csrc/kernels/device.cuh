@@ -251,13 +251,53 @@ struct MomFlux {
 // its four edges: 1/h (approximate reciprocal) and sqrt(h).
 __device__ __forceinline__ float rcp_depth(float h) { return __fdividef(1.f, h); }
 
+// Constants of the 2s momentum flux that depend only on the edge's row (its
+// metrics), the step's dt and the scenario's viscosity: the deep-water kernels
+// form them once per row of a unit, the general kernel per edge, with the same
+// expressions, so both paths give the same fluxes.
+struct XRowK {
+    float ilcos;   // len / cos of the row
+    float kdes;    // cd * val * ilcos, val = 2 ilcos dt / (area0 + area1), cd = (1 - cvis) / 2
+};
+__device__ __forceinline__ XRowK make_xrow(float ilcos, float asum, float dt, float cvis)
+{
+    XRowK k;
+    const float val = (2.f * ilcos * dt) / asum;
+    k.ilcos = ilcos;
+    k.kdes = (0.5f * (1.f - cvis)) * val * ilcos;
+    return k;
+}
+struct YRowK {
+    float len, cmid, cdiff, c10;   // len; (cos0 + cos1) / 2; cos1 - cos0; cos1 / cos0
+    float c01, li0, kdes0, kdes1;  // cos0 / cos1; len / cos0; cd val len / cos0; cd val len / cos1
+    float cos0, cos1;
+};
+__device__ __forceinline__ YRowK make_yrow(float cos0, float cos1, float icos0, float icos1, float len, float asum,
+                                           float dt, float cvis)
+{
+    YRowK k;
+    const float val = (2.f * len * dt) / asum;
+    const float kd = (0.5f * (1.f - cvis)) * val * len;
+    k.len = len;
+    k.cmid = 0.5f * (cos0 + cos1);
+    k.cdiff = cos1 - cos0;
+    k.c10 = cos1 * icos0;
+    k.c01 = cos0 * icos1;
+    k.li0 = len * icos0;
+    k.kdes0 = kd * icos0;
+    k.kdes1 = kd * icos1;
+    k.cos0 = cos0;
+    k.cos1 = cos1;
+    return k;
+}
+
 // x edge, components (qx, qy); u = qx normal, v = qy tangential, rh = 1/h,
-// sh = sqrt(h) of each side, jump = the surface jump, asum = area0 + area1
+// sh = sqrt(h) of each side, jump = the surface jump, k = the row's constants
 // (src/GPU/Arista_kernel.cu:221-464, alfa = 1)
 __device__ __forceinline__ void momentum_2s_x(MomFlux &r, float h0, float h1, float rh0, float rh1, float s0, float s1,
-                                              float u0, float u1, float v0, float v1, float jump, float ilcos,
-                                              float asum, float dt, float cvis)
+                                              float u0, float u1, float v0, float v1, float jump, const XRowK &k)
 {
+    const float ilcos = k.ilcos;
     const float hij = 0.5f * (h0 + h1);
     const float u0n = u0 * rh0, u1n = u1 * rh1;
     const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
@@ -270,42 +310,35 @@ __device__ __forceinline__ void momentum_2s_x(MomFlux &r, float h0, float h1, fl
         mx = u0n * u0 * ilcos; px = -mx; mx += hij * jump * ilcos;
         my = u0n * v0 * ilcos; py = -my;
     }
-    const float cd = 0.5f * (1.f - cvis);
-    const float val = (2.f * ilcos * dt) / asum;
-    const float des = cd * val * maxa * maxa * (u1 - u0) * ilcos;
+    const float des = k.kdes * (maxa * maxa) * (u1 - u0);
     r.m_x = mx - des; r.m_y = my;
     r.p_x = px + des; r.p_y = py;
     r.lam = ilcos * maxa;
     r.active = true;
 }
 
-// y edge, components (qx, qy); u = qy normal, v = qx tangential; icos =
-// 1/cos(lat) of each side's row, correctly rounded
-// (src/GPU/Arista_kernel.cu:780-1026, alfa = 1)
+// y edge, components (qx, qy); u = qy normal, v = qx tangential; k = the
+// constants of the edge's row pair (src/GPU/Arista_kernel.cu:780-1026, alfa = 1)
 __device__ __forceinline__ void momentum_2s_y(MomFlux &r, float h0, float h1, float rh0, float rh1, float s0, float s1,
-                                              float u0, float u1, float v0, float v1, float jump, float cos0,
-                                              float cos1, float icos0, float icos1, float len, float asum, float dt,
-                                              float cvis)
+                                              float u0, float u1, float v0, float v1, float jump, const YRowK &k)
 {
     const float hij = 0.5f * (h0 + h1);
     const float u0n = u0 * rh0, u1n = u1 * rh1;
     const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
     const float maxa = fabsf(uijn) + sqrtf(hij);
-    const float deta = 0.5f * (cos0 + cos1) * jump - uijn * uijn * (cos1 - cos0);
+    const float deta = k.cmid * jump - uijn * uijn * k.cdiff;
     float fym, fyp, fxm, fxp;
     if (uijn < 0.f) {
-        fym = u1n * u1 * len; fyp = -fym; fym *= cos1 * icos0; fym += hij * deta * len * icos0;
-        fxm = u1n * v1 * len; fxp = -fxm;
+        fym = u1n * u1 * k.len; fyp = -fym; fym *= k.c10; fym += hij * deta * k.li0;
+        fxm = u1n * v1 * k.len; fxp = -fxm;
     } else {
-        fym = u0n * u0 * len; fyp = -fym * cos0 * icos1; fym += hij * deta * len * icos0;
-        fxm = u0n * v0 * len; fxp = -fxm;
+        fym = u0n * u0 * k.len; fyp = -fym * k.c01; fym += hij * deta * k.li0;
+        fxm = u0n * v0 * k.len; fxp = -fxm;
     }
-    const float val = (2.f * len * dt) / asum;
-    const float cd = 0.5f * (1.f - cvis);
-    const float des = cd * val * maxa * maxa * (u1 * cos1 - u0 * cos0) * len;
-    r.m_x = fxm; r.m_y = fym - des * icos0;
-    r.p_x = fxp; r.p_y = fyp + des * icos1;
-    r.lam = len * maxa;
+    const float m2 = (maxa * maxa) * (u1 * k.cos1 - u0 * k.cos0);
+    r.m_x = fxm; r.m_y = fym - k.kdes0 * m2;
+    r.p_x = fxp; r.p_y = fyp + k.kdes1 * m2;
+    r.lam = k.len * maxa;
     r.active = true;
 }
 
@@ -378,7 +411,7 @@ __device__ __forceinline__ MomFlux momentum_flux_x(Edge &e, const ScenarioDev &s
     const float ilcos = e.len;
     if (all_deep(e, s.hpos)) {
         momentum_2s_x(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrtf(e.h0), sqrtf(e.h1), e.u0, e.u1, e.v0,
-                      e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1), ilcos, e.area0 + e.area1, dt, s.cvis);
+                      e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1), make_xrow(ilcos, e.area0 + e.area1, dt, s.cvis));
         return r;
     }
     if (e.front) swap_sides(e);
@@ -469,8 +502,9 @@ __device__ __forceinline__ MomFlux momentum_flux_y(Edge &e, const ScenarioDev &s
     const float len = e.len;
     if (all_deep(e, s.hpos)) {
         momentum_2s_y(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrtf(e.h0), sqrtf(e.h1), e.u0, e.u1, e.v0,
-                      e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1), e.cos0, e.cos1, __frcp_rn(e.cos0),
-                      __frcp_rn(e.cos1), len, e.area0 + e.area1, dt, s.cvis);
+                      e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1),
+                      make_yrow(e.cos0, e.cos1, __frcp_rn(e.cos0), __frcp_rn(e.cos1), len, e.area0 + e.area1, dt,
+                                s.cvis));
         return r;
     }
     if (e.front) swap_sides(e);

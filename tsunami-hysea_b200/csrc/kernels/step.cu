@@ -471,8 +471,13 @@ __host__ __device__ constexpr size_t deep_stage_bytes(int phase)
 struct DeepRow {
     float4 m;      // cos, ilcos, area, dlon (edge row)
     float icos;    // 1/cos, correctly rounded
-    float pad[3];
+    // phase 2, for the unit's dt: dt / area, 1 / (2 cfl area), the x edges'
+    // XRowK::kdes, and the YRowK of the y edge above the row (y0: len, cmid,
+    // cdiff, c10; y1: c01, li0, kdes0, kdes1)
+    float dtA, kcfl, kdx;
+    float4 y0, y1;
 };
+static_assert(sizeof(DeepRow) == 64, "row metrics: four float4");
 __host__ __device__ constexpr size_t deep_misc_offset(int phase) { return 2 * deep_stage_bytes(phase); }
 static size_t deep_smem_bytes(int phase, int ng)
 {
@@ -559,21 +564,25 @@ __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2
 }
 
 // y edge between rows gy-1 (a, row metrics ra) and gy (b, rb) of a deep tile;
-// phase 2 also takes 1/h and sqrt(h) of both cells
+// phase 2 also takes 1/h and sqrt(h) of both cells, and the edge's constants
+// from rb
 template <int PHASE>
 __device__ __forceinline__ void y_edge_deep(const ScenarioDev &s, const Cell &a, const Cell &b, float rha, float sha,
                                             float rhb, float shb, const DeepRow &ra, const DeepRow &rb, float dt,
                                             Contrib &lo, Contrib &hi)
 {
-    const float cos0 = ra.m.x, cos1 = rb.m.x, area0 = ra.m.z, area1 = rb.m.z, len = rb.m.w;
+    const float cos0 = ra.m.x, cos1 = rb.m.x;
     if (PHASE == 1) {
-        const float F = mass_2s_y(a.qy, len, cos0, cos1, a.h, b.h, dt, area0, area1);
+        const float F = mass_2s_y(a.qy, rb.m.w, cos0, cos1, a.h, b.h, dt, ra.m.z, rb.m.z);
         lo = {-F / cos0, 0.f, 0.f};
         hi = {F / cos1, 0.f, 0.f};
     } else {
+        YRowK k;
+        k.len = rb.y0.x; k.cmid = rb.y0.y; k.cdiff = rb.y0.z; k.c10 = rb.y0.w;
+        k.c01 = rb.y1.x; k.li0 = rb.y1.y; k.kdes0 = rb.y1.z; k.kdes1 = rb.y1.w;
+        k.cos0 = cos0; k.cos1 = cos1;
         MomFlux f;
-        momentum_2s_y(f, a.h, b.h, rha, rhb, sha, shb, a.qy, b.qy, a.qx, b.qx, surface_jump(a.e, b.e, a.D, b.D), cos0,
-                      cos1, ra.icos, rb.icos, len, area0 + area1, dt, s.cvis);
+        momentum_2s_y(f, a.h, b.h, rha, rhb, sha, shb, a.qy, b.qy, a.qx, b.qx, surface_jump(a.e, b.e, a.D, b.D), k);
         lo = {-f.m_x, -f.m_y, f.lam};
         hi = {-f.p_x, -f.p_y, f.lam};
     }
@@ -685,11 +694,23 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
         ScenarioCtl *ctl = s.ctl;
         const int x0 = d.x0, yb = d.yb, p = d.p;
         if (d.run) {
-            // row metrics of the window while the copies are in flight
+            const float dt = (float)ctl->dt;
+            // row metrics of the window (phase 2: with the unit's dt folded
+            // in) while the copies are in flight
             if (threadIdx.x < kStageRows) {
                 DeepRow r;
                 r.m = __ldg(s.rowpack + yb - 1 + threadIdx.x);
                 r.icos = __frcp_rn(r.m.x);
+                if (PHASE == 2) {
+                    // the row above (a deep unit is at least two rows below the top)
+                    const float4 a = __ldg(s.rowpack + max(yb - 2 + (int)threadIdx.x, 0));
+                    r.dtA = __fdividef(dt, r.m.z);
+                    r.kcfl = 1.f / (2.f * s.cfl * r.m.z);
+                    r.kdx = make_xrow(r.m.y, r.m.z + r.m.z, dt, s.cvis).kdes;
+                    const YRowK k = make_yrow(a.x, r.m.x, __frcp_rn(a.x), r.icos, r.m.w, a.z + r.m.z, dt, s.cvis);
+                    r.y0 = make_float4(k.len, k.cmid, k.cdiff, k.c10);
+                    r.y1 = make_float4(k.c01, k.li0, k.kdes0, k.kdes1);
+                }
                 rows[threadIdx.x] = r;
             }
             const bool ok = mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u);
@@ -703,7 +724,6 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 return;
             }
             const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
-            const float dt = (float)ctl->dt;
             const float t_sec = (float)(ctl->t * ctl->T);
             const int pitch = s.pitch;
             const int r_first = row0 + 1;                           // staged row of this warp's first output row
@@ -711,8 +731,8 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
             const int gx = x0 - 4 + sc;                             // grid column
             const bool has_cell = (lane >= 2) && (lane <= 29);
             const int dcol = strip * 28 - 2 + lane;                 // diagnostics column (cells only)
-            float local_min = FLT_MAX;    // phase 1: depth minimum; phase 2: dt
-            float local_max = -FLT_MAX;   // phase 1: depth maximum
+            float local_min = FLT_MAX;    // phase 1: depth minimum
+            float local_max = -FLT_MAX;   // phase 1: depth maximum; phase 2: max of lam / (2 cfl area)
             bool bad = false;
             int i = r_first * kStageW + sc;
             Cell c = staged_cell(stage, i);
@@ -759,8 +779,8 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                     const float e0 = stage[i - 1], D0 = stage[SPLANE + i - 1];
                     MomFlux f;
                     momentum_2s_x(f, e0 + D0, c.h, shup(rh_c, 1), rh_c, shup(sh_c, 1), sh_c, stage[2 * SPLANE + i - 1],
-                                  c.qx, stage[3 * SPLANE + i - 1], c.qy, surface_jump(e0, c.e, D0, c.D), rc.m.y,
-                                  area + area, dt, s.cvis);
+                                  c.qx, stage[3 * SPLANE + i - 1], c.qy, surface_jump(e0, c.e, D0, c.D),
+                                  XRowK{rc.m.y, rc.kdx});
                     xl = {-f.m_x, -f.m_y, f.lam};
                     xr = {-f.p_x, -f.p_y, f.lam};
                 }
@@ -787,11 +807,12 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                         local_min = fminf(local_min, eta + c.D);
                         local_max = fmaxf(local_max, eta + c.D);
                     } else {
-                        // momentum update; no sponge, filter or friction in a deep tile
+                        // momentum update; no sponge, filter or friction in a deep tile.
+                        // The cell's dt bound 2 cfl area / lam (1e30 for lam < eps)
+                        // is taken as the unit's largest lam / (2 cfl area), inverted once.
                         const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
-                        const float step = (lam < kEps) ? 1e30f : __fdividef(2.f * s.cfl * area, lam);
-                        local_min = fminf(local_min, step);
-                        const float val = __fdividef(dt, area);
+                        local_max = fmaxf(local_max, (lam < kEps) ? 0.f : lam * rc.kcfl);
+                        const float val = rc.dtA;
                         const float qx = c.qx + val * (((xr.a + xrr.a) + top.a) + below.a);
                         const float qy = c.qy + val * (((xr.b + xrr.b) + top.b) + below.b);
                         if (!isfinite(qx) || !isfinite(qy)) bad = true;
@@ -807,9 +828,10 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
             }
             if (bad) atomicOr(&ctl->errors, 1u);
             for (int o = 16; o > 0; o >>= 1) {
-                local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
-                if (PHASE == 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+                if (PHASE == 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+                local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
             }
+            if (PHASE == 2) local_min = (local_max > 0.f) ? 1.f / local_max : 1e30f;
             if (lane == 0) {
                 red[warp] = local_min;
                 if (PHASE == 1) red[NW + warp] = local_max;
