@@ -756,6 +756,8 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
             float *out0 = (PHASE == 1) ? s.eta[p ^ 1] : s.qx[p ^ 1];
             float *out1 = s.qy[p ^ 1];
             int off = (yb + r_first - 1) * pitch + gx;
+            // running sum of the cells' new values: non-finite iff one of them is
+            float fin = 0.f;
             for (int k = 0; k < nrows; k++, i += kStageW, off += pitch) {
                 const DeepRow rn = rows[r_first + k + 1];
                 const Cell n = staged_cell(stage, i + kStageW);
@@ -791,34 +793,33 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                     xrr.b = shdn(xl.b, 1);
                     xrr.lam = shdn(xl.lam, 1);
                 }
-                if (has_cell) {
-                    if (PHASE == 1) {
-                        // diagnostics of the state the step starts from (src/GPU/Metrics.cu:23-77)
-                        const float *dg = stage + 4 * SPLANE + (r_first - 1 + k) * kTileX + dcol;
-                        const float em = dg[0], ar = dg[DPLANE], ei = dg[2 * DPLANE];
-                        if (c.e > em && c.h > s.eps_h) s.eta_max[off] = c.e;
-                        if (ar < 0.f && fabsf(c.e - ei) > s.dif_at) s.arr[off] = t_sec;
-                        // mass update (src/GPU/Volumen_kernel.cu:111-157)
-                        const float acc = ((xr.a + xrr.a) + top.a) + below.a;
-                        float eta = c.e + __fdividef(dt, area) * acc;
-                        if (!(eta + c.D > 0.f)) eta = -c.D;
-                        if (!isfinite(eta)) bad = true;
-                        out0[off] = eta;
-                        local_min = fminf(local_min, eta + c.D);
-                        local_max = fmaxf(local_max, eta + c.D);
-                    } else {
-                        // momentum update; no sponge, filter or friction in a deep tile.
-                        // The cell's dt bound 2 cfl area / lam (1e30 for lam < eps)
-                        // is taken as the unit's largest lam / (2 cfl area), inverted once.
-                        const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
-                        local_max = fmaxf(local_max, (lam < kEps) ? 0.f : lam * rc.kcfl);
-                        const float val = rc.dtA;
-                        const float qx = c.qx + val * (((xr.a + xrr.a) + top.a) + below.a);
-                        const float qy = c.qy + val * (((xr.b + xrr.b) + top.b) + below.b);
-                        if (!isfinite(qx) || !isfinite(qy)) bad = true;
-                        out0[off] = qx;
-                        out1[off] = qy;
-                    }
+                if (PHASE == 1 && has_cell) {
+                    // diagnostics of the state the step starts from (src/GPU/Metrics.cu:23-77)
+                    const float *dg = stage + 4 * SPLANE + (r_first - 1 + k) * kTileX + dcol;
+                    const float em = dg[0], ar = dg[DPLANE], ei = dg[2 * DPLANE];
+                    if (c.e > em && c.h > s.eps_h) s.eta_max[off] = c.e;
+                    if (ar < 0.f && fabsf(c.e - ei) > s.dif_at) s.arr[off] = t_sec;
+                    // mass update (src/GPU/Volumen_kernel.cu:111-157)
+                    const float acc = ((xr.a + xrr.a) + top.a) + below.a;
+                    float eta = c.e + __fdividef(dt, area) * acc;
+                    if (!(eta + c.D > 0.f)) eta = -c.D;
+                    fin += eta;
+                    out0[off] = eta;
+                    local_min = fminf(local_min, eta + c.D);
+                    local_max = fmaxf(local_max, eta + c.D);
+                } else if (PHASE == 2 && has_cell) {
+                    // momentum update; no sponge, filter or friction in a deep
+                    // tile.  The cell's dt bound 2 cfl area / lam (1e30 for
+                    // lam < eps) is taken as the unit's largest lam / (2 cfl
+                    // area), inverted once per unit.
+                    const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
+                    local_max = fmaxf(local_max, (lam < kEps) ? 0.f : lam * rc.kcfl);
+                    const float val = rc.dtA;
+                    const float qx = c.qx + val * (((xr.a + xrr.a) + top.a) + below.a);
+                    const float qy = c.qy + val * (((xr.b + xrr.b) + top.b) + below.b);
+                    fin += qx + qy;
+                    out0[off] = qx;
+                    out1[off] = qy;
                 }
                 top = next_top;
                 rc = rn;
@@ -826,21 +827,24 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 rh_c = rh_n;
                 sh_c = sh_n;
             }
+            if (!isfinite(fin)) bad = true;
             if (bad) atomicOr(&ctl->errors, 1u);
             for (int o = 16; o > 0; o >>= 1) {
                 if (PHASE == 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
                 local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
             }
-            if (PHASE == 2) local_min = (local_max > 0.f) ? 1.f / local_max : 1e30f;
             if (lane == 0) {
-                red[warp] = local_min;
+                red[warp] = (PHASE == 1) ? local_min : local_max;
                 if (PHASE == 1) red[NW + warp] = local_max;
             }
         }
         __syncthreads();   // every warp is done with the staged window and the row metrics
         if (d.run && threadIdx.x == 0) {
             float m = red[0];
-            for (int k = 1; k < NW; k++) m = fminf(m, red[k]);
+            for (int k = 1; k < NW; k++) m = (PHASE == 1) ? fminf(m, red[k]) : fmaxf(m, red[k]);
+            // phase 2: the unit's dt bound from its largest lam / (2 cfl area),
+            // inverted once per unit so that it does not depend on the warps' rows
+            if (PHASE == 2) m = (m > 0.f) ? 1.f / m : 1e30f;
             if (PHASE == 1) {
                 // a deep unit reports its whole-unit {min, max} for its strips
                 // and corners too: conservative for a neighbour's deep test,
@@ -1120,6 +1124,13 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
             warp_unit_summary(hacc, cell, cell && gx < ux0 + 2, cell && gx >= ux1 - 2, slots + 9 * warp);
         } else {
             for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+            if (PHASE == 2) {
+                // one atomic per warp and no barrier: the minimum is exact in
+                // any order, and the warps of a CTA go on to their next unit
+                // without waiting for the slowest
+                if (lane == 0) atomicMin(&ctl->dt_bits, __float_as_uint(local_min));
+                continue;
+            }
             if (lane == 0) red[warp] = local_min;
         }
         __syncthreads();
