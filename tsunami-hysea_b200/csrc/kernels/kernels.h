@@ -45,6 +45,7 @@ struct StepLaunch {
     const int2 *work;          // work list: (scenario slot, tile)
     const int *nwork;          // its length (device)
     int *lists;                // deep / general lists of the step: 2 counts + 2 x cap indices
+    int *claims;               // units claimed beyond the first wave by deep phase 1 / 2 (zeroed by classification)
     int cap;                   // list capacity (>= work-list length)
     int grid;                  // general kernel grid
     int deep_grid[2];          // persistent deep kernel grids, phase 1 and 2

@@ -462,8 +462,10 @@ static_assert(kTileY == 2 * kHalfRows, "two half tiles per tile");
 static_assert((SPLANE * 4) % 128 == 0 && (DPLANE * 4) % 128 == 0, "staged planes 128-byte aligned");
 
 // Shared memory of a deep kernel CTA: two staging buffers (double buffering
-// across work units), then the two mbarriers, the staged row metrics of the
-// current unit and the reduction scratch.
+// across work units), then the two mbarriers, the claimed next unit (its
+// index and descriptor), the staged row metrics of the current unit and the
+// reduction scratch.
+constexpr size_t kNextBytes = 48;
 __host__ __device__ constexpr size_t deep_stage_bytes(int phase)
 {
     return (size_t)(4 * SPLANE + (phase == 1 ? 3 * DPLANE : 0)) * sizeof(float);
@@ -481,7 +483,7 @@ static_assert(sizeof(DeepRow) == 64, "row metrics: four float4");
 __host__ __device__ constexpr size_t deep_misc_offset(int phase) { return 2 * deep_stage_bytes(phase); }
 static size_t deep_smem_bytes(int phase, int ng)
 {
-    return deep_misc_offset(phase) + 16 + kStageRows * sizeof(DeepRow) + 2 * 4 * ng * sizeof(float);
+    return deep_misc_offset(phase) + 16 + kNextBytes + kStageRows * sizeof(DeepRow) + 2 * 4 * ng * sizeof(float);
 }
 
 // one cell of a staged row (shared memory; the depth is formed here)
@@ -514,9 +516,13 @@ __device__ __forceinline__ const int *general_items(const int *lists, int cap) {
 // the grid (the lower half of a last tile row of <= 16 rows) are not listed.
 // The counts are zeroed before the launch.
 __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int before_step)
+                                const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int before_step,
+                                int *__restrict__ claims)
 {
     const int n = 2 * *nwork_ptr;
+    // the deep kernels that read these lists claim units from zero (the
+    // previous ones are done: this kernel runs after phase 1)
+    if (blockIdx.x == 0 && threadIdx.x < 2) claims[threadIdx.x] = 0;
     const int lane = threadIdx.x & 31;
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int u = base + threadIdx.x;
@@ -594,6 +600,7 @@ struct DeepUnit {
     int uidx, x0, yb, p;      // uidx: the unit's index in the scenario's unit grid
     bool run;
 };
+static_assert(sizeof(DeepUnit) + 16 <= kNextBytes, "claimed unit's slot in shared memory");
 
 __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                               const int *__restrict__ lists, int i)
@@ -647,13 +654,16 @@ __device__ __forceinline__ void deep_issue(const DeepUnit &d, float *stage, uint
 // output columns, lanes 2..29) with a two-row window.
 template <int PHASE, int NG, int MINB>
 __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                                   const int *__restrict__ lists)
+                                                   const int *__restrict__ lists, int *__restrict__ claim)
 {
     extern __shared__ __align__(1024) unsigned char dsm[];
     constexpr size_t SB = deep_stage_bytes(PHASE);
     // staging buffer b at dsm + b * SB
     uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + deep_misc_offset(PHASE));
-    DeepRow *rows = reinterpret_cast<DeepRow *>(dsm + deep_misc_offset(PHASE) + 16);
+    // the unit thread 0 claimed for the next iteration: its index and descriptor
+    int &s_next = *reinterpret_cast<int *>(dsm + deep_misc_offset(PHASE) + 16);
+    DeepUnit &s_unit = *reinterpret_cast<DeepUnit *>(dsm + deep_misc_offset(PHASE) + 32);
+    DeepRow *rows = reinterpret_cast<DeepRow *>(dsm + deep_misc_offset(PHASE) + 16 + kNextBytes);
     float *red = reinterpret_cast<float *>(rows + kStageRows);   // per warp: dt, or depth min and max
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     constexpr int NW = 4 * NG;
@@ -680,15 +690,24 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
     DeepUnit d = deep_unit(scen, work, lists, blockIdx.x);
     if (threadIdx.x == 0 && d.run) deep_issue<PHASE>(d, reinterpret_cast<float *>(dsm), &bars[0], acq);
     int buf = 0;
-    for (int u = blockIdx.x; u < nunits; u += gridDim.x, buf ^= 1) {
+    // The first two waves take units blockIdx.x and blockIdx.x + gridDim.x;
+    // after that each CTA claims its units from the counter (2 gridDim.x,
+    // 2 gridDim.x + 1, ...), so a CTA that started late, or whose units took
+    // longer, takes fewer.  Thread 0 claims one unit ahead of the copy it
+    // issues (the claim's latency hides behind a unit's compute); the other
+    // threads learn the next unit at the next barrier.
+    int pending = blockIdx.x + gridDim.x;   // thread 0: the unit after the current one
+    for (int u = blockIdx.x; u < nunits; buf ^= 1) {
         // the next unit's copy goes to the other buffer, free since the end of the previous unit
-        const int un = u + gridDim.x;
-        DeepUnit dn;
-        dn.run = false;
-        if (un < nunits) {
-            dn = deep_unit(scen, work, lists, un);
-            if (threadIdx.x == 0 && dn.run)
-                deep_issue<PHASE>(dn, reinterpret_cast<float *>(dsm + (buf ^ 1) * SB), &bars[buf ^ 1], acq);
+        if (threadIdx.x == 0) {
+            const int un = pending;
+            s_next = un;
+            if (un < nunits) {
+                const DeepUnit dn = deep_unit(scen, work, lists, un);
+                s_unit = dn;
+                if (dn.run) deep_issue<PHASE>(dn, reinterpret_cast<float *>(dsm + (buf ^ 1) * SB), &bars[buf ^ 1], acq);
+                pending = 2 * (int)gridDim.x + atomicAdd(claim, 1);
+            }
         }
         const ScenarioDev &s = *d.s;
         ScenarioCtl *ctl = s.ctl;
@@ -720,7 +739,8 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 // copies one more bounded wait so none is still writing, stop
                 if (threadIdx.x == 0) atomicOr(&ctl->errors, 2u);
                 mbar_wait_bounded(&bars[buf], ((phase_bits >> buf) & 1u) ^ 1u);
-                if (dn.run) mbar_wait_bounded(&bars[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u);
+                const int un = s_next;   // written before the barrier above
+                if (un < nunits && s_unit.run) mbar_wait_bounded(&bars[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u);
                 return;
             }
             const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
@@ -839,6 +859,8 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
             }
         }
         __syncthreads();   // every warp is done with the staged window and the row metrics
+        const int un = s_next;
+        const DeepUnit dn = s_unit;   // valid when un < nunits
         if (d.run && threadIdx.x == 0) {
             float m = red[0];
             for (int k = 1; k < NW; k++) m = (PHASE == 1) ? fminf(m, red[k]) : fmaxf(m, red[k]);
@@ -858,7 +880,8 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 atomicAdd(&ctl->units_deep, 1ull);
             }
         }
-        __syncthreads();   // red[] is reused by the next unit
+        __syncthreads();   // red[] and s_next are reused by the next unit
+        u = un;
         d = dn;
     }
 }
@@ -1172,7 +1195,8 @@ static void launch_deep(const StepLaunch &L, cudaStream_t st)
 {
     constexpr int NG = deep_ng(PHASE, V);
     deep_kernel<PHASE, NG, deep_minb(PHASE, V)>
-        <<<L.deep_grid[PHASE - 1], 128 * NG, deep_smem_bytes(PHASE, NG), st>>>(L.scen, L.work, L.lists);
+        <<<L.deep_grid[PHASE - 1], 128 * NG, deep_smem_bytes(PHASE, NG), st>>>(L.scen, L.work, L.lists,
+                                                                            L.claims + (PHASE - 1));
 }
 template <int PHASE>
 static void launch_deep_any(const StepLaunch &L, cudaStream_t st)
@@ -1200,7 +1224,7 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
     case 1: launch_general<1>(L, st); break;
     case 2:
         cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
-        classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0);
+        classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0, L.claims);
         break;
     case 3: launch_deep_any<2>(L, st); break;
     case 4: launch_general<2>(L, st); break;
@@ -1217,7 +1241,7 @@ void launch_initial_dt(const StepLaunch &L, cudaStream_t st)
 void launch_lists_current(const StepLaunch &L, cudaStream_t st)
 {
     cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
-    classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 1);
+    classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 1, L.claims);
 }
 
 template <int PHASE, int V>

@@ -669,6 +669,7 @@ Batch::~Batch()
     if (d_work0) cudaFreeAsync(d_work0, st);
     if (d_nwork0) cudaFreeAsync(d_nwork0, st);
     if (d_lists) cudaFreeAsync(d_lists, st);
+    if (d_claims) cudaFreeAsync(d_claims, st);
     if (d_ctl) cudaFreeAsync(d_ctl, st);
     cudaFreeHost(h_ctl);
     if (ev0) cudaEventDestroy(ev0);
@@ -693,6 +694,8 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     THY_CK(cudaMallocAsync(&d_nwork0, sizeof(int), st));
     THY_CK(cudaMallocAsync(&d_lists, (2 + 4 * (size_t)std::max(max_work, 1)) * sizeof(int), st));
     THY_CK(cudaMemsetAsync(d_lists, 0, 2 * sizeof(int), st));
+    THY_CK(cudaMallocAsync(&d_claims, 2 * sizeof(int), st));
+    THY_CK(cudaMemsetAsync(d_claims, 0, 2 * sizeof(int), st));
     THY_CK(cudaEventCreate(&ev0));
     THY_CK(cudaEventCreate(&ev1));
     THY_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
@@ -840,6 +843,7 @@ StepLaunch Batch::params() const
     L.work = d_work;
     L.nwork = d_nwork;
     L.lists = d_lists;
+    L.claims = d_claims;
     L.cap = 2 * work_capacity;   // lists hold work units (two per work-list entry)
     L.tiling = tiling;
     // general kernel: a grid of 8 waves of resident CTAs striding over the

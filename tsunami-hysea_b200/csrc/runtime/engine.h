@@ -104,6 +104,7 @@ struct Batch {
     int2 *d_work0 = nullptr;           // work list of scenarios joining (their initial dt)
     int *d_nwork0 = nullptr;
     int *d_lists = nullptr;            // deep / general lists of the current step (StepLaunch::lists)
+    int *d_claims = nullptr;           // StepLaunch::claims
     ScenarioCtl *d_ctl = nullptr;      // slots
     ScenarioCtl *h_ctl = nullptr;      // pinned mirror
     int capacity = 0;
