@@ -444,6 +444,16 @@ __device__ __forceinline__ void tma_load_2d(float *dst, const TmaMap *map, int x
         : "memory");
 }
 
+// untiled bulk copy global -> shared (no multicast): both addresses 16-byte
+// aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+        ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar))
+        : "memory");
+}
+
 __device__ __forceinline__ void tmap_acquire(const TmaMap *map)
 {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(map) : "memory");
@@ -466,9 +476,19 @@ static_assert((SPLANE * 4) % 128 == 0 && (DPLANE * 4) % 128 == 0, "staged planes
 // index and descriptor), the staged row metrics of the current unit and the
 // reduction scratch.
 constexpr size_t kNextBytes = 48;
-__host__ __device__ constexpr size_t deep_stage_bytes(int phase)
+// A phase-1 staging buffer also receives the unit's packed row metrics, rows
+// yb-2 .. yb+16 (a deep unit lies at least two rows inside the grid), copied
+// with the planes so that they arrive one unit ahead too; phase 2 derives its
+// row constants from them while its copies are in flight.
+constexpr int kRawRows = kStageRows + 1;
+constexpr uint32_t kRawRowBytes = kRawRows * 16;
+__host__ __device__ constexpr size_t deep_raw_rows_offset(int phase)
 {
     return (size_t)(4 * SPLANE + (phase == 1 ? 3 * DPLANE : 0)) * sizeof(float);
+}
+__host__ __device__ constexpr size_t deep_stage_bytes(int phase)
+{
+    return deep_raw_rows_offset(phase) + (phase == 1 ? (kRawRowBytes + 127) / 128 * 128 : 0);   // 128-byte aligned
 }
 struct DeepRow {
     float4 m;      // cos, ilcos, area, dlon (edge row)
@@ -633,7 +653,10 @@ __device__ __forceinline__ void deep_issue(const DeepUnit &d, float *stage, uint
         for (int k = 0; k < kNumMaps; k++) tmap_acquire(m + k);
         acq = m;
     }
-    mbar_expect_tx(bar, 4 * kStateBytes + (PHASE == 1 ? 3 * kDiagBytes : 0));
+    mbar_expect_tx(bar, 4 * kStateBytes + (PHASE == 1 ? 3 * kDiagBytes + kRawRowBytes : 0));
+    if (PHASE == 1)
+        bulk_load(reinterpret_cast<unsigned char *>(stage) + deep_raw_rows_offset(PHASE), d.s->rowpack + d.yb - 2,
+                  kRawRowBytes, bar);
     tma_load_2d(stage, m + me, d.x0 - 4, d.yb - 1, bar);
     tma_load_2d(stage + SPLANE, m + kMapDep, d.x0 - 4, d.yb - 1, bar);
     tma_load_2d(stage + 2 * SPLANE, m + kMapQx0 + p, d.x0 - 4, d.yb - 1, bar);
@@ -714,22 +737,20 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
         const int x0 = d.x0, yb = d.yb, p = d.p;
         if (d.run) {
             const float dt = (float)ctl->dt;
-            // row metrics of the window (phase 2: with the unit's dt folded
-            // in) while the copies are in flight
-            if (threadIdx.x < kStageRows) {
+            if (PHASE == 2 && threadIdx.x < kStageRows) {
+                // row constants of the window with the unit's dt folded in,
+                // while the copies are in flight; staged row t is grid row
+                // yb - 1 + t
                 DeepRow r;
                 r.m = __ldg(s.rowpack + yb - 1 + threadIdx.x);
+                const float4 a = __ldg(s.rowpack + yb - 2 + threadIdx.x);   // the row above
                 r.icos = __frcp_rn(r.m.x);
-                if (PHASE == 2) {
-                    // the row above (a deep unit is at least two rows below the top)
-                    const float4 a = __ldg(s.rowpack + max(yb - 2 + (int)threadIdx.x, 0));
-                    r.dtA = __fdividef(dt, r.m.z);
-                    r.kcfl = 1.f / (2.f * s.cfl * r.m.z);
-                    r.kdx = make_xrow(r.m.y, r.m.z + r.m.z, dt, s.cvis).kdes;
-                    const YRowK k = make_yrow(a.x, r.m.x, __frcp_rn(a.x), r.icos, r.m.w, a.z + r.m.z, dt, s.cvis);
-                    r.y0 = make_float4(k.len, k.cmid, k.cdiff, k.c10);
-                    r.y1 = make_float4(k.c01, k.li0, k.kdes0, k.kdes1);
-                }
+                r.dtA = __fdividef(dt, r.m.z);
+                r.kcfl = 1.f / (2.f * s.cfl * r.m.z);
+                r.kdx = make_xrow(r.m.y, r.m.z + r.m.z, dt, s.cvis).kdes;
+                const YRowK k = make_yrow(a.x, r.m.x, __frcp_rn(a.x), r.icos, r.m.w, a.z + r.m.z, dt, s.cvis);
+                r.y0 = make_float4(k.len, k.cmid, k.cdiff, k.c10);
+                r.y1 = make_float4(k.c01, k.li0, k.kdes0, k.kdes1);
                 rows[threadIdx.x] = r;
             }
             const bool ok = mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u);
@@ -743,6 +764,15 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 if (un < nunits && s_unit.run) mbar_wait_bounded(&bars[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u);
                 return;
             }
+            // phase 1: the row metrics as staged (row t of the window at t + 1)
+            const float4 *rowm =
+                reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE)) + 1;
+            auto row = [&](int t) {
+                if (PHASE == 2) return rows[t];
+                DeepRow r;
+                r.m = rowm[t];
+                return r;
+            };
             const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
             const float t_sec = (float)(ctl->t * ctl->T);
             const int pitch = s.pitch;
@@ -761,7 +791,7 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 rh_c = rcp_depth(c.h);
                 sh_c = sqrtf(c.h);
             }
-            DeepRow rc = rows[r_first];
+            DeepRow rc = row(r_first);
             Contrib top;
             {
                 const Cell a = staged_cell(stage, i - kStageW);
@@ -771,7 +801,7 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                     sh_a = sqrtf(a.h);
                 }
                 Contrib dummy;
-                y_edge_deep<PHASE>(s, a, c, rh_a, sh_a, rh_c, sh_c, rows[r_first - 1], rc, dt, dummy, top);
+                y_edge_deep<PHASE>(s, a, c, rh_a, sh_a, rh_c, sh_c, row(r_first - 1), rc, dt, dummy, top);
             }
             float *out0 = (PHASE == 1) ? s.eta[p ^ 1] : s.qx[p ^ 1];
             float *out1 = s.qy[p ^ 1];
@@ -779,7 +809,7 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
             // running sum of the cells' new values: non-finite iff one of them is
             float fin = 0.f;
             for (int k = 0; k < nrows; k++, i += kStageW, off += pitch) {
-                const DeepRow rn = rows[r_first + k + 1];
+                const DeepRow rn = row(r_first + k + 1);
                 const Cell n = staged_cell(stage, i + kStageW);
                 const float area = rc.m.z;
                 float rh_n = 0.f, sh_n = 0.f;
