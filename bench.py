@@ -288,7 +288,7 @@ def run_ours(a, dist: Dist):
             times.append(time.perf_counter() - t0)
             steps_run = out["iterations"]
             parts.append((out["setup_seconds"], out["loop_seconds"], out["device_ms"] / 1e3, out["output_seconds"],
-                          out["total_seconds"]))
+                          out["total_seconds"], out["release_seconds"]))
         t = dist.max(statistics.mean(times))
         e2e = {"value": round(dist.sum(float(cells * steps_run)) / t, 1), "unit": METRIC,
                "h2d_bytes_per_step": int(32 * cells + 4 * (5 * p.ny + 1) + 80 * len(p.faults)),
@@ -299,7 +299,8 @@ def run_ours(a, dist: Dist):
                "loop_s": round(statistics.mean(x[1] for x in parts), 4),
                "loop_device_s": round(statistics.mean(x[2] for x in parts), 4),
                "output_s": round(statistics.mean(x[3] for x in parts), 4),
-               "library_call_s": round(statistics.mean(x[4] for x in parts), 4)}
+               "library_call_s": round(statistics.mean(x[4] for x in parts), 4),
+               "release_s": round(statistics.mean(x[5] for x in parts), 4)}
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not a.skip_cpu:
         try:

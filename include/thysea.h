@@ -138,6 +138,7 @@ typedef struct thy_stats {
     double total_seconds;     /* the whole call, release of the device buffers included */
     thy_tiling tiling;        /* the warp tiling of the loop's last chunk */
     long long tune_samples;   /* chunks of the loop timed for the autotuner */
+    double release_seconds;   /* release of the device buffers, graphs and streams after the outputs */
 } thy_stats;
 
 /* Library / device. */

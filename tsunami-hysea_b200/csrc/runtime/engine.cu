@@ -19,8 +19,10 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <map>
 #include <mutex>
 #include <thread>
+#include <unordered_map>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -66,6 +68,60 @@ int ensure_device()
 }
 
 int device_sm_count() { return g_sms[g_device] > 0 ? g_sms[g_device] : 148; }
+
+// Page-locked host blocks reused across runs.  Pinning and unpinning are
+// driver calls that synchronise the device, and unpinning a block was seen to
+// stall a run's release for over half a second; freed blocks are kept by
+// power-of-two size class (up to kPinnedKeep bytes in all) and handed out
+// again.  Blocks are portable: any device of the process may copy to them.
+namespace {
+constexpr size_t kPinnedKeep = (size_t)2 << 30;
+std::mutex g_pin_mu;
+std::multimap<size_t, void *> g_pin_free;          // size class -> free block
+std::unordered_map<void *, size_t> g_pin_class;    // every block handed out -> its size class
+size_t g_pin_kept = 0;
+}  // namespace
+
+cudaError_t pinned_alloc(void **p, size_t bytes)
+{
+    size_t cls = 4096;
+    while (cls < bytes) cls <<= 1;
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto it = g_pin_free.find(cls);
+        if (it != g_pin_free.end()) {
+            *p = it->second;
+            g_pin_free.erase(it);
+            g_pin_kept -= cls;
+            g_pin_class[*p] = cls;
+            return cudaSuccess;
+        }
+    }
+    const cudaError_t e = cudaHostAlloc(p, cls, cudaHostAllocPortable);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lk(g_pin_mu);
+    g_pin_class[*p] = cls;
+    return cudaSuccess;
+}
+
+void pinned_free(void *p)
+{
+    if (!p) return;
+    {
+        std::lock_guard<std::mutex> lk(g_pin_mu);
+        auto it = g_pin_class.find(p);
+        if (it != g_pin_class.end()) {
+            const size_t cls = it->second;
+            g_pin_class.erase(it);
+            if (g_pin_kept + cls <= kPinnedKeep) {
+                g_pin_free.emplace(cls, p);
+                g_pin_kept += cls;
+                return;
+            }
+        }
+    }
+    cudaFreeHost(p);
+}
 
 static int round_up(int a, int b) { return (a + b - 1) / b * b; }
 
@@ -418,8 +474,8 @@ public:
         }
         if (d_snap1_) cudaFreeAsync(d_snap1_, alloc_st_);
         if (d_ts_) cudaFreeAsync(d_ts_, alloc_st_);
-        cudaFreeHost(h_snap_);
-        cudaFreeHost(h_ts_);
+        pinned_free(h_snap_);
+        pinned_free(h_ts_);
         if (copy_st_) cudaStreamDestroy(copy_st_);
     }
 
@@ -433,7 +489,7 @@ public:
         THY_CK(cudaStreamCreateWithFlags(&copy_st_, cudaStreamNonBlocking));
         if (o && o->on_snapshot && s->save_nc >= 0.0) {
             THY_CK(cudaMallocAsync(&d_snap1_, 3 * n_ * sizeof(float), st));
-            THY_CK(cudaMallocHost(&h_snap_, kSnapSlots * 3 * n_ * sizeof(float)));
+            THY_CK(pinned_alloc(reinterpret_cast<void **>(&h_snap_), kSnapSlots * 3 * n_ * sizeof(float)));
             for (int k = 0; k < kSnapSlots; k++) {
                 THY_CK(cudaEventCreateWithFlags(&snap_ready_[k], cudaEventDisableTiming));
                 THY_CK(cudaEventCreateWithFlags(&snap_copied_[k], cudaEventDisableTiming));
@@ -441,7 +497,7 @@ public:
         }
         if (np_ > 0) {
             THY_CK(cudaMallocAsync(&d_ts_, kTsSlots * 4 * (size_t)np_ * sizeof(float), st));
-            THY_CK(cudaMallocHost(&h_ts_, kTsSlots * 4 * (size_t)np_ * sizeof(float)));
+            THY_CK(pinned_alloc(reinterpret_cast<void **>(&h_ts_), kTsSlots * 4 * (size_t)np_ * sizeof(float)));
             for (int k = 0; k < kTsSlots; k++) {
                 THY_CK(cudaEventCreateWithFlags(&ts_ready_[k], cudaEventDisableTiming));
                 THY_CK(cudaEventCreateWithFlags(&ts_copied_[k], cudaEventDisableTiming));
@@ -671,7 +727,7 @@ Batch::~Batch()
     if (d_lists) cudaFreeAsync(d_lists, st);
     if (d_claims) cudaFreeAsync(d_claims, st);
     if (d_ctl) cudaFreeAsync(d_ctl, st);
-    cudaFreeHost(h_ctl);
+    pinned_free(h_ctl);
     if (ev0) cudaEventDestroy(ev0);
     if (ev1) cudaEventDestroy(ev1);
     if (ev_fork) cudaEventDestroy(ev_fork);
@@ -687,7 +743,7 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     THY_CK(cudaGetDevice(&device));
     THY_CK(cudaMallocAsync(&d_table, cap * sizeof(ScenarioDev), st));
     THY_CK(cudaMallocAsync(&d_ctl, cap * sizeof(ScenarioCtl), st));
-    THY_CK(cudaMallocHost(&h_ctl, cap * sizeof(ScenarioCtl)));
+    THY_CK(pinned_alloc(reinterpret_cast<void **>(&h_ctl), cap * sizeof(ScenarioCtl)));
     THY_CK(cudaMallocAsync(&d_work, std::max(max_work, 1) * sizeof(int2), st));
     THY_CK(cudaMallocAsync(&d_nwork, sizeof(int), st));
     THY_CK(cudaMallocAsync(&d_work0, std::max(max_work, 1) * sizeof(int2), st));
@@ -1096,6 +1152,7 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
     cudaStream_t st;
     THY_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     auto t0 = std::chrono::steady_clock::now();
+    auto t_release = t0;
     {
         DevScenario s;
         Batch b;
@@ -1148,10 +1205,15 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
             if (stats)
                 stats->output_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t2).count();
         }
-    out:;
+    out:
+        t_release = std::chrono::steady_clock::now();
     }
     cudaStreamDestroy(st);
-    if (stats) stats->total_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_start).count();
+    if (stats) {
+        const auto t_end = std::chrono::steady_clock::now();
+        stats->release_seconds = std::chrono::duration<double>(t_end - t_release).count();
+        stats->total_seconds = std::chrono::duration<double>(t_end - t_start).count();
+    }
     return rc;
 }
 

@@ -149,5 +149,8 @@ struct Batch {
 
 int ensure_device();
 int device_sm_count();
+// page-locked host blocks, reused across runs (engine.cu)
+cudaError_t pinned_alloc(void **p, size_t bytes);
+void pinned_free(void *p);
 
 }  // namespace thy

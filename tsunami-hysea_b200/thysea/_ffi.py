@@ -73,7 +73,7 @@ class Stats(ctypes.Structure):
         ("kernel_launches", ctypes.c_longlong), ("snapshots", ctypes.c_int), ("series_samples", ctypes.c_int),
         ("tiles", ctypes.c_longlong), ("deep_tiles", ctypes.c_longlong), ("dry_tiles", ctypes.c_longlong),
         ("setup_seconds", ctypes.c_double), ("output_seconds", ctypes.c_double), ("total_seconds", ctypes.c_double),
-        ("tiling", Tiling), ("tune_samples", ctypes.c_longlong),
+        ("tiling", Tiling), ("tune_samples", ctypes.c_longlong), ("release_seconds", ctypes.c_double),
     ]
 
 
