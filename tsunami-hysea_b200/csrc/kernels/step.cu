@@ -472,10 +472,11 @@ static_assert(kTileY == 2 * kHalfRows, "two half tiles per tile");
 static_assert((SPLANE * 4) % 128 == 0 && (DPLANE * 4) % 128 == 0, "staged planes 128-byte aligned");
 
 // Shared memory of a deep kernel CTA: two staging buffers (double buffering
-// across work units), then the two mbarriers, the claimed next unit (its
-// index and descriptor), the staged row metrics of the current unit and the
-// reduction scratch.
-constexpr size_t kNextBytes = 48;
+// across work units), then the two mbarriers, the claimed next unit (index
+// and descriptor, one slot per buffer parity) and the error flag, the staged
+// row metrics of the current unit and the reduction scratch (one set per
+// buffer parity).
+constexpr size_t kNextBytes = 80;   // s_next[2], s_err, pad, s_unit[2]
 // A phase-1 staging buffer also receives the unit's packed row metrics, rows
 // yb-2 .. yb+16 (a deep unit lies at least two rows inside the grid), copied
 // with the planes so that they arrive one unit ahead too; phase 2 derives its
@@ -503,7 +504,7 @@ static_assert(sizeof(DeepRow) == 64, "row metrics: four float4");
 __host__ __device__ constexpr size_t deep_misc_offset(int phase) { return 2 * deep_stage_bytes(phase); }
 static size_t deep_smem_bytes(int phase, int ng)
 {
-    return deep_misc_offset(phase) + 16 + kNextBytes + kStageRows * sizeof(DeepRow) + 2 * 4 * ng * sizeof(float);
+    return deep_misc_offset(phase) + 16 + kNextBytes + kStageRows * sizeof(DeepRow) + 2 * 2 * 4 * ng * sizeof(float);
 }
 
 // one cell of a staged row (shared memory; the depth is formed here)
@@ -620,7 +621,7 @@ struct DeepUnit {
     int uidx, x0, yb, p;      // uidx: the unit's index in the scenario's unit grid
     bool run;
 };
-static_assert(sizeof(DeepUnit) + 16 <= kNextBytes, "claimed unit's slot in shared memory");
+static_assert(2 * sizeof(DeepUnit) + 16 <= kNextBytes, "claimed units' slots in shared memory");
 
 __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                               const int *__restrict__ lists, int i)
@@ -668,74 +669,85 @@ __device__ __forceinline__ void deep_issue(const DeepUnit &d, float *stage, uint
     }
 }
 
-// Phase 1 / 2 of the deep tiles, persistent: CTA b steps units b, b + grid,
-// ... of the deep list (two per tile: its upper and lower half).  A unit's
-// window - its rows plus one above and one below, columns x0-4 .. x0+115 of
-// eta, dep, qx, qy, and in phase 1 the diagnostics of its own cells - is
-// staged by TMA, the next unit's copy in flight while the current one is
-// computed.  Warp w marches its row group (w >> 2) of column strip w & 3 (28
-// output columns, lanes 2..29) with a two-row window.
+// Phase 1 / 2 of the deep tiles, persistent, over the units of the deep list
+// (two per tile: its upper and lower half).  A unit's window - its rows plus
+// one above and one below, columns x0-4 .. x0+115 of eta, dep, qx, qy, and in
+// phase 1 the diagnostics of its own cells and the row metrics - is staged by
+// TMA, the next unit's copy in flight while the current one is computed.
+// Compute warp w marches its row group (w >> 2) of column strip w & 3 (28
+// output columns, lanes 2..29) with a two-row window; one more warp is the
+// producer.
 template <int PHASE, int NG, int MINB>
-__global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                                   const int *__restrict__ lists, int *__restrict__ claim)
+__global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const ScenarioDev *__restrict__ scen,
+                                                                const int2 *__restrict__ work,
+                                                                const int *__restrict__ lists, int *__restrict__ claim)
 {
     extern __shared__ __align__(1024) unsigned char dsm[];
     constexpr size_t SB = deep_stage_bytes(PHASE);
+    constexpr int NW = 4 * NG;      // compute warps
+    constexpr int PT = NW * 32;     // the producer: lane 0 of warp NW
     // staging buffer b at dsm + b * SB
-    uint64_t *bars = reinterpret_cast<uint64_t *>(dsm + deep_misc_offset(PHASE));
-    // the unit thread 0 claimed for the next iteration: its index and descriptor
-    int &s_next = *reinterpret_cast<int *>(dsm + deep_misc_offset(PHASE) + 16);
-    DeepUnit &s_unit = *reinterpret_cast<DeepUnit *>(dsm + deep_misc_offset(PHASE) + 32);
-    DeepRow *rows = reinterpret_cast<DeepRow *>(dsm + deep_misc_offset(PHASE) + 16 + kNextBytes);
-    float *red = reinterpret_cast<float *>(rows + kStageRows);   // per warp: dt, or depth min and max
+    unsigned char *misc = dsm + deep_misc_offset(PHASE);
+    uint64_t *bars = reinterpret_cast<uint64_t *>(misc);
+    int *s_next = reinterpret_cast<int *>(misc + 16);          // [parity]: the unit after the current one
+    int &s_err = *reinterpret_cast<int *>(misc + 24);          // a copy did not land in time
+    DeepUnit *s_unit = reinterpret_cast<DeepUnit *>(misc + 32);   // [parity]: its descriptor
+    DeepRow *rows = reinterpret_cast<DeepRow *>(misc + 16 + kNextBytes);
+    float *red0 = reinterpret_cast<float *>(rows + kStageRows);   // [parity][2 NW]: per warp dt, or depth min and max
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    constexpr int NW = 4 * NG;
+    const bool producer = warp == NW;
     const int strip = warp & 3, group = warp >> 2;
-    // this warp's rows of the unit: kHalfRows * group / NG .. kHalfRows * (group + 1) / NG - 1
+    // a compute warp's rows of the unit: kHalfRows * group / NG .. kHalfRows * (group + 1) / NG - 1
     const int row0 = kHalfRows * group / NG, nrows = kHalfRows * (group + 1) / NG - row0;
     const int nunits = lists[0];
     if (blockIdx.x >= nunits) return;
     // TMA destinations must be 128-byte aligned: a misaligned buffer is
     // reported on every scenario of the CTA's units and nothing is copied
     if (smem_addr(dsm) & 127u) {
-        if (threadIdx.x == 0)
+        if (threadIdx.x == PT)
             for (int u = blockIdx.x; u < nunits; u += gridDim.x)
                 atomicOr(&scen[work[deep_items(lists)[u] >> 1].x].ctl->errors, 4u);
         return;
     }
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == PT) {
         mbar_init(&bars[0]);
         mbar_init(&bars[1]);
+        s_err = 0;
     }
     __syncthreads();
     uint32_t phase_bits = 0;     // bit b: parity of the next completion of bars[b]
-    const TmaMap *acq = nullptr; // maps acquired by this CTA (thread 0)
+    const TmaMap *acq = nullptr; // maps acquired by this CTA (producer)
     DeepUnit d = deep_unit(scen, work, lists, blockIdx.x);
-    if (threadIdx.x == 0 && d.run) deep_issue<PHASE>(d, reinterpret_cast<float *>(dsm), &bars[0], acq);
+    if (threadIdx.x == PT && d.run) deep_issue<PHASE>(d, reinterpret_cast<float *>(dsm), &bars[0], acq);
     int buf = 0;
     // The first two waves take units blockIdx.x and blockIdx.x + gridDim.x;
     // after that each CTA claims its units from the counter (2 gridDim.x,
     // 2 gridDim.x + 1, ...), so a CTA that started late, or whose units took
-    // longer, takes fewer.  Thread 0 claims one unit ahead of the copy it
-    // issues (the claim's latency hides behind a unit's compute); the other
-    // threads learn the next unit at the next barrier.
-    int pending = blockIdx.x + gridDim.x;   // thread 0: the unit after the current one
+    // longer, takes fewer.  A producer warp claims the units, reads their
+    // descriptors, issues their copies one unit ahead and reduces each unit's
+    // results, while the compute warps step the current unit; they meet once
+    // per unit, and the producer publishes the next unit there.
+    int pending = blockIdx.x + gridDim.x;   // producer: the unit after the next one
     for (int u = blockIdx.x; u < nunits; buf ^= 1) {
-        // the next unit's copy goes to the other buffer, free since the end of the previous unit
-        if (threadIdx.x == 0) {
-            const int un = pending;
-            s_next = un;
-            if (un < nunits) {
-                const DeepUnit dn = deep_unit(scen, work, lists, un);
-                s_unit = dn;
-                if (dn.run) deep_issue<PHASE>(dn, reinterpret_cast<float *>(dsm + (buf ^ 1) * SB), &bars[buf ^ 1], acq);
-                pending = 2 * (int)gridDim.x + atomicAdd(claim, 1);
+        float *red = red0 + buf * 2 * NW;
+        if (producer) {
+            // the next unit's copy goes to the other buffer, free since the
+            // compute warps passed the end of the previous unit
+            if (lane == 0) {
+                const int un = pending;
+                s_next[buf ^ 1] = un;
+                if (un < nunits) {
+                    const DeepUnit dn = deep_unit(scen, work, lists, un);
+                    s_unit[buf ^ 1] = dn;
+                    if (dn.run)
+                        deep_issue<PHASE>(dn, reinterpret_cast<float *>(dsm + (buf ^ 1) * SB), &bars[buf ^ 1], acq);
+                    pending = 2 * (int)gridDim.x + atomicAdd(claim, 1);
+                }
             }
-        }
-        const ScenarioDev &s = *d.s;
-        ScenarioCtl *ctl = s.ctl;
-        const int x0 = d.x0, yb = d.yb, p = d.p;
-        if (d.run) {
+        } else if (d.run) {
+            const ScenarioDev &s = *d.s;
+            ScenarioCtl *ctl = s.ctl;
+            const int x0 = d.x0, yb = d.yb, p = d.p;
             const float dt = (float)ctl->dt;
             if (PHASE == 2 && threadIdx.x < kStageRows) {
                 // row constants of the window with the unit's dt folded in,
@@ -753,145 +765,155 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 r.y1 = make_float4(k.c01, k.li0, k.kdes0, k.kdes1);
                 rows[threadIdx.x] = r;
             }
-            const bool ok = mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u);
-            phase_bits ^= 1u << buf;
-            if (__syncthreads_or(!ok)) {
-                // the copies did not land in time: report, give both buffers'
-                // copies one more bounded wait so none is still writing, stop
-                if (threadIdx.x == 0) atomicOr(&ctl->errors, 2u);
-                mbar_wait_bounded(&bars[buf], ((phase_bits >> buf) & 1u) ^ 1u);
-                const int un = s_next;   // written before the barrier above
-                if (un < nunits && s_unit.run) mbar_wait_bounded(&bars[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u);
-                return;
-            }
-            // phase 1: the row metrics as staged (row t of the window at t + 1)
-            const float4 *rowm =
-                reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE)) + 1;
-            auto row = [&](int t) {
-                if (PHASE == 2) return rows[t];
-                DeepRow r;
-                r.m = rowm[t];
-                return r;
-            };
-            const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
-            const float t_sec = (float)(ctl->t * ctl->T);
-            const int pitch = s.pitch;
-            const int r_first = row0 + 1;                           // staged row of this warp's first output row
-            const int sc = strip * 28 + 2 + lane;                   // staged column of this lane
-            const int gx = x0 - 4 + sc;                             // grid column
-            const bool has_cell = (lane >= 2) && (lane <= 29);
-            const int dcol = strip * 28 - 2 + lane;                 // diagnostics column (cells only)
-            float local_min = FLT_MAX;    // phase 1: depth minimum
-            float local_max = -FLT_MAX;   // phase 1: depth maximum; phase 2: max of lam / (2 cfl area)
-            bool bad = false;
-            int i = r_first * kStageW + sc;
-            Cell c = staged_cell(stage, i);
-            float rh_c = 0.f, sh_c = 0.f;
-            if (PHASE == 2) {
-                rh_c = rcp_depth(c.h);
-                sh_c = sqrtf(c.h);
-            }
-            DeepRow rc = row(r_first);
-            Contrib top;
-            {
-                const Cell a = staged_cell(stage, i - kStageW);
-                float rh_a = 0.f, sh_a = 0.f;
+            if (!mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u)) s_err = 1;
+            // the compute warps only: the row constants are written, every copy checked
+            asm volatile("bar.sync 1, %0;" ::"r"(PT) : "memory");
+            if (!s_err) {
+                // phase 1: the row metrics as staged (row t of the window at t + 1)
+                const float4 *rowm =
+                    reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE)) + 1;
+                auto row = [&](int t) {
+                    if (PHASE == 2) return rows[t];
+                    DeepRow r;
+                    r.m = rowm[t];
+                    return r;
+                };
+                const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
+                const float t_sec = (float)(ctl->t * ctl->T);
+                const int pitch = s.pitch;
+                const int r_first = row0 + 1;                           // staged row of this warp's first output row
+                const int sc = strip * 28 + 2 + lane;                   // staged column of this lane
+                const int gx = x0 - 4 + sc;                             // grid column
+                const bool has_cell = (lane >= 2) && (lane <= 29);
+                const int dcol = strip * 28 - 2 + lane;                 // diagnostics column (cells only)
+                float local_min = FLT_MAX;    // phase 1: depth minimum
+                float local_max = -FLT_MAX;   // phase 1: depth maximum; phase 2: max of lam / (2 cfl area)
+                bool bad = false;
+                int i = r_first * kStageW + sc;
+                Cell c = staged_cell(stage, i);
+                float rh_c = 0.f, sh_c = 0.f;
                 if (PHASE == 2) {
-                    rh_a = rcp_depth(a.h);
-                    sh_a = sqrtf(a.h);
+                    rh_c = rcp_depth(c.h);
+                    sh_c = sqrtf(c.h);
                 }
-                Contrib dummy;
-                y_edge_deep<PHASE>(s, a, c, rh_a, sh_a, rh_c, sh_c, row(r_first - 1), rc, dt, dummy, top);
-            }
-            float *out0 = (PHASE == 1) ? s.eta[p ^ 1] : s.qx[p ^ 1];
-            float *out1 = s.qy[p ^ 1];
-            int off = (yb + r_first - 1) * pitch + gx;
-            // running sum of the cells' new values: non-finite iff one of them is
-            float fin = 0.f;
-            for (int k = 0; k < nrows; k++, i += kStageW, off += pitch) {
-                const DeepRow rn = row(r_first + k + 1);
-                const Cell n = staged_cell(stage, i + kStageW);
-                const float area = rc.m.z;
-                float rh_n = 0.f, sh_n = 0.f;
-                if (PHASE == 2) {
-                    rh_n = rcp_depth(n.h);
-                    sh_n = sqrtf(n.h);
+                DeepRow rc = row(r_first);
+                Contrib top;
+                {
+                    const Cell a = staged_cell(stage, i - kStageW);
+                    float rh_a = 0.f, sh_a = 0.f;
+                    if (PHASE == 2) {
+                        rh_a = rcp_depth(a.h);
+                        sh_a = sqrtf(a.h);
+                    }
+                    Contrib dummy;
+                    y_edge_deep<PHASE>(s, a, c, rh_a, sh_a, rh_c, sh_c, row(r_first - 1), rc, dt, dummy, top);
                 }
-                // y edge below this row
-                Contrib below, next_top;
-                y_edge_deep<PHASE>(s, c, n, rh_c, sh_c, rh_n, sh_n, rc, rn, dt, below, next_top);
-                // x edge left of this lane's cell
-                Contrib xl, xr;
-                if (PHASE == 1) {
-                    const float F = mass_2s_x(stage[2 * SPLANE + i - 1], rc.m.y, stage[i - 1] + stage[SPLANE + i - 1],
-                                              c.h, dt, area, area);
-                    xl = {-F, 0.f, 0.f};
-                    xr = {F, 0.f, 0.f};
-                } else {
-                    const float e0 = stage[i - 1], D0 = stage[SPLANE + i - 1];
-                    MomFlux f;
-                    momentum_2s_x(f, e0 + D0, c.h, shup(rh_c, 1), rh_c, shup(sh_c, 1), sh_c, stage[2 * SPLANE + i - 1],
-                                  c.qx, stage[3 * SPLANE + i - 1], c.qy, surface_jump(e0, c.e, D0, c.D),
-                                  XRowK{rc.m.y, rc.kdx});
-                    xl = {-f.m_x, -f.m_y, f.lam};
-                    xr = {-f.p_x, -f.p_y, f.lam};
+                float *out0 = (PHASE == 1) ? s.eta[p ^ 1] : s.qx[p ^ 1];
+                float *out1 = s.qy[p ^ 1];
+                int off = (yb + r_first - 1) * pitch + gx;
+                // running sum of the cells' new values: non-finite iff one of them is
+                float fin = 0.f;
+                for (int k = 0; k < nrows; k++, i += kStageW, off += pitch) {
+                    const DeepRow rn = row(r_first + k + 1);
+                    const Cell n = staged_cell(stage, i + kStageW);
+                    const float area = rc.m.z;
+                    float rh_n = 0.f, sh_n = 0.f;
+                    if (PHASE == 2) {
+                        rh_n = rcp_depth(n.h);
+                        sh_n = sqrtf(n.h);
+                    }
+                    // y edge below this row
+                    Contrib below, next_top;
+                    y_edge_deep<PHASE>(s, c, n, rh_c, sh_c, rh_n, sh_n, rc, rn, dt, below, next_top);
+                    // x edge left of this lane's cell
+                    Contrib xl, xr;
+                    if (PHASE == 1) {
+                        const float F = mass_2s_x(stage[2 * SPLANE + i - 1], rc.m.y, stage[i - 1] + stage[SPLANE + i - 1],
+                                                  c.h, dt, area, area);
+                        xl = {-F, 0.f, 0.f};
+                        xr = {F, 0.f, 0.f};
+                    } else {
+                        const float e0 = stage[i - 1], D0 = stage[SPLANE + i - 1];
+                        MomFlux f;
+                        momentum_2s_x(f, e0 + D0, c.h, shup(rh_c, 1), rh_c, shup(sh_c, 1), sh_c, stage[2 * SPLANE + i - 1],
+                                      c.qx, stage[3 * SPLANE + i - 1], c.qy, surface_jump(e0, c.e, D0, c.D),
+                                      XRowK{rc.m.y, rc.kdx});
+                        xl = {-f.m_x, -f.m_y, f.lam};
+                        xr = {-f.p_x, -f.p_y, f.lam};
+                    }
+                    // the right edge of this cell is the left edge of lane+1
+                    Contrib xrr;
+                    xrr.a = shdn(xl.a, 1);
+                    if (PHASE == 2) {
+                        xrr.b = shdn(xl.b, 1);
+                        xrr.lam = shdn(xl.lam, 1);
+                    }
+                    if (PHASE == 1 && has_cell) {
+                        // diagnostics of the state the step starts from (src/GPU/Metrics.cu:23-77)
+                        const float *dg = stage + 4 * SPLANE + (r_first - 1 + k) * kTileX + dcol;
+                        const float em = dg[0], ar = dg[DPLANE], ei = dg[2 * DPLANE];
+                        if (c.e > em && c.h > s.eps_h) s.eta_max[off] = c.e;
+                        if (ar < 0.f && fabsf(c.e - ei) > s.dif_at) s.arr[off] = t_sec;
+                        // mass update (src/GPU/Volumen_kernel.cu:111-157)
+                        const float acc = ((xr.a + xrr.a) + top.a) + below.a;
+                        float eta = c.e + __fdividef(dt, area) * acc;
+                        if (!(eta + c.D > 0.f)) eta = -c.D;
+                        fin += eta;
+                        out0[off] = eta;
+                        local_min = fminf(local_min, eta + c.D);
+                        local_max = fmaxf(local_max, eta + c.D);
+                    } else if (PHASE == 2 && has_cell) {
+                        // momentum update; no sponge, filter or friction in a deep
+                        // tile.  The cell's dt bound 2 cfl area / lam (1e30 for
+                        // lam < eps) is taken as the unit's largest lam / (2 cfl
+                        // area), inverted once per unit.
+                        const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
+                        local_max = fmaxf(local_max, (lam < kEps) ? 0.f : lam * rc.kcfl);
+                        const float val = rc.dtA;
+                        const float qx = c.qx + val * (((xr.a + xrr.a) + top.a) + below.a);
+                        const float qy = c.qy + val * (((xr.b + xrr.b) + top.b) + below.b);
+                        fin += qx + qy;
+                        out0[off] = qx;
+                        out1[off] = qy;
+                    }
+                    top = next_top;
+                    rc = rn;
+                    c = n;
+                    rh_c = rh_n;
+                    sh_c = sh_n;
                 }
-                // the right edge of this cell is the left edge of lane+1
-                Contrib xrr;
-                xrr.a = shdn(xl.a, 1);
-                if (PHASE == 2) {
-                    xrr.b = shdn(xl.b, 1);
-                    xrr.lam = shdn(xl.lam, 1);
+                if (!isfinite(fin)) bad = true;
+                if (bad) atomicOr(&ctl->errors, 1u);
+                for (int o = 16; o > 0; o >>= 1) {
+                    if (PHASE == 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+                    local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
                 }
-                if (PHASE == 1 && has_cell) {
-                    // diagnostics of the state the step starts from (src/GPU/Metrics.cu:23-77)
-                    const float *dg = stage + 4 * SPLANE + (r_first - 1 + k) * kTileX + dcol;
-                    const float em = dg[0], ar = dg[DPLANE], ei = dg[2 * DPLANE];
-                    if (c.e > em && c.h > s.eps_h) s.eta_max[off] = c.e;
-                    if (ar < 0.f && fabsf(c.e - ei) > s.dif_at) s.arr[off] = t_sec;
-                    // mass update (src/GPU/Volumen_kernel.cu:111-157)
-                    const float acc = ((xr.a + xrr.a) + top.a) + below.a;
-                    float eta = c.e + __fdividef(dt, area) * acc;
-                    if (!(eta + c.D > 0.f)) eta = -c.D;
-                    fin += eta;
-                    out0[off] = eta;
-                    local_min = fminf(local_min, eta + c.D);
-                    local_max = fmaxf(local_max, eta + c.D);
-                } else if (PHASE == 2 && has_cell) {
-                    // momentum update; no sponge, filter or friction in a deep
-                    // tile.  The cell's dt bound 2 cfl area / lam (1e30 for
-                    // lam < eps) is taken as the unit's largest lam / (2 cfl
-                    // area), inverted once per unit.
-                    const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
-                    local_max = fmaxf(local_max, (lam < kEps) ? 0.f : lam * rc.kcfl);
-                    const float val = rc.dtA;
-                    const float qx = c.qx + val * (((xr.a + xrr.a) + top.a) + below.a);
-                    const float qy = c.qy + val * (((xr.b + xrr.b) + top.b) + below.b);
-                    fin += qx + qy;
-                    out0[off] = qx;
-                    out1[off] = qy;
+                if (lane == 0) {
+                    red[warp] = (PHASE == 1) ? local_min : local_max;
+                    if (PHASE == 1) red[NW + warp] = local_max;
                 }
-                top = next_top;
-                rc = rn;
-                c = n;
-                rh_c = rh_n;
-                sh_c = sh_n;
-            }
-            if (!isfinite(fin)) bad = true;
-            if (bad) atomicOr(&ctl->errors, 1u);
-            for (int o = 16; o > 0; o >>= 1) {
-                if (PHASE == 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
-                local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
-            }
-            if (lane == 0) {
-                red[warp] = (PHASE == 1) ? local_min : local_max;
-                if (PHASE == 1) red[NW + warp] = local_max;
             }
         }
-        __syncthreads();   // every warp is done with the staged window and the row metrics
-        const int un = s_next;
-        const DeepUnit dn = s_unit;   // valid when un < nunits
-        if (d.run && threadIdx.x == 0) {
+        if (d.run) phase_bits ^= 1u << buf;
+        // every compute warp is done with the staged window, the row metrics
+        // and its results; the next unit and the error flag are published
+        __syncthreads();
+        if (s_err) {
+            // a copy did not land in time: report; the producer gives both
+            // buffers' copies one more bounded wait so none is still writing; stop
+            if (threadIdx.x == PT) {
+                atomicOr(&d.s->ctl->errors, 2u);
+                mbar_wait_bounded(&bars[buf], ((phase_bits >> buf) & 1u) ^ 1u);
+                if (s_next[buf ^ 1] < nunits && s_unit[buf ^ 1].run)
+                    mbar_wait_bounded(&bars[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u);
+            }
+            return;
+        }
+        const int un = s_next[buf ^ 1];
+        const DeepUnit dn = s_unit[buf ^ 1];   // valid when un < nunits
+        if (d.run && threadIdx.x == PT) {
+            const ScenarioDev &s = *d.s;
+            ScenarioCtl *ctl = s.ctl;
             float m = red[0];
             for (int k = 1; k < NW; k++) m = (PHASE == 1) ? fminf(m, red[k]) : fmaxf(m, red[k]);
             // phase 2: the unit's dt bound from its largest lam / (2 cfl area),
@@ -904,13 +926,12 @@ __global__ void __launch_bounds__(128 * NG, MINB) deep_kernel(const ScenarioDev 
                 float mx = red[NW];
                 for (int k = 1; k < NW; k++) mx = fmaxf(mx, red[NW + k]);
                 const float2 v = make_float2(m, mx);
-                s.usum[p ^ 1][d.uidx] = UnitSum{v, v, v, v, v, v, v, v, v};
+                s.usum[d.p ^ 1][d.uidx] = UnitSum{v, v, v, v, v, v, v, v, v};
             } else {
                 atomicMin(&ctl->dt_bits, __float_as_uint(m));
                 atomicAdd(&ctl->units_deep, 1ull);
             }
         }
-        __syncthreads();   // red[] and s_next are reused by the next unit
         u = un;
         d = dn;
     }
@@ -1225,7 +1246,7 @@ static void launch_deep(const StepLaunch &L, cudaStream_t st)
 {
     constexpr int NG = deep_ng(PHASE, V);
     deep_kernel<PHASE, NG, deep_minb(PHASE, V)>
-        <<<L.deep_grid[PHASE - 1], 128 * NG, deep_smem_bytes(PHASE, NG), st>>>(L.scen, L.work, L.lists,
+        <<<L.deep_grid[PHASE - 1], 128 * NG + 32, deep_smem_bytes(PHASE, NG), st>>>(L.scen, L.work, L.lists,
                                                                             L.claims + (PHASE - 1));
 }
 template <int PHASE>
@@ -1310,7 +1331,7 @@ static int deep_occupancy()
 {
     constexpr int NG = deep_ng(PHASE, V);
     int n = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<PHASE, NG, deep_minb(PHASE, V)>, 128 * NG,
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, deep_kernel<PHASE, NG, deep_minb(PHASE, V)>, 128 * NG + 32,
                                                   deep_smem_bytes(PHASE, NG));
     return n;
 }
