@@ -536,7 +536,9 @@ __device__ __forceinline__ const int *general_items(const int *lists, int cap) {
 // changed has unknown (NaN) summaries, so its units are general.  Units below
 // the grid (the lower half of a last tile row of <= 16 rows) are not listed.
 // The counts are zeroed before the launch.
-__global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
+constexpr int kClassifyThreads = 256, kClassifyWarps = kClassifyThreads / 32;
+__global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const ScenarioDev *__restrict__ scen,
+                                                                   const int2 *__restrict__ work,
                                 const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int before_step,
                                 int *__restrict__ claims)
 {
@@ -544,7 +546,9 @@ __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2
     // the deep kernels that read these lists claim units from zero (the
     // previous ones are done: this kernel runs after phase 1)
     if (blockIdx.x == 0 && threadIdx.x < 2) claims[threadIdx.x] = 0;
-    const int lane = threadIdx.x & 31;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    __shared__ int cnt[2][kClassifyWarps];   // per warp: deep and general units of this round
+    __shared__ int base2[2];                 // the block's first deep and general list slots
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int u = base + threadIdx.x;
         bool listed = false, deep = false;
@@ -572,21 +576,32 @@ __global__ void classify_kernel(const ScenarioDev *__restrict__ scen, const int2
                 }
             }
         }
-        // warp-aggregated appends
+        // block-aggregated appends: one atomic per list and block (the
+        // counters are two words that every block appends to)
         const unsigned dm = __ballot_sync(0xffffffffu, listed && deep);
         const unsigned gm = __ballot_sync(0xffffffffu, listed && !deep);
-        int dbase = 0, gbase = 0;
         if (lane == 0) {
-            if (dm) dbase = atomicAdd(&lists[0], __popc(dm));
-            if (gm) gbase = atomicAdd(&lists[1], __popc(gm));
+            cnt[0][warp] = __popc(dm);
+            cnt[1][warp] = __popc(gm);
         }
-        dbase = __shfl_sync(0xffffffffu, dbase, 0);
-        gbase = __shfl_sync(0xffffffffu, gbase, 0);
+        __syncthreads();
+        if (threadIdx.x < 2) {
+            int tot = 0;
+            for (int w = 0; w < kClassifyWarps; w++) tot += cnt[threadIdx.x][w];
+            base2[threadIdx.x] = tot ? atomicAdd(&lists[threadIdx.x], tot) : 0;
+        }
+        __syncthreads();
+        int dbase = base2[0], gbase = base2[1];
+        for (int w = 0; w < warp; w++) {
+            dbase += cnt[0][w];
+            gbase += cnt[1][w];
+        }
         const unsigned below = (1u << lane) - 1u;
         if (listed) {
             if (deep) lists[2 + dbase + __popc(dm & below)] = u;
             else lists[2 + cap + gbase + __popc(gm & below)] = u;
         }
+        __syncthreads();   // cnt and base2 are reused by the next round
     }
 }
 
@@ -1275,7 +1290,7 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
     case 1: launch_general<1>(L, st); break;
     case 2:
         cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
-        classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0, L.claims);
+        classify_kernel<<<L.classify_grid, kClassifyThreads, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 0, L.claims);
         break;
     case 3: launch_deep_any<2>(L, st); break;
     case 4: launch_general<2>(L, st); break;
@@ -1292,7 +1307,7 @@ void launch_initial_dt(const StepLaunch &L, cudaStream_t st)
 void launch_lists_current(const StepLaunch &L, cudaStream_t st)
 {
     cudaMemsetAsync(L.lists, 0, 2 * sizeof(int), st);
-    classify_kernel<<<L.classify_grid, 256, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 1, L.claims);
+    classify_kernel<<<L.classify_grid, kClassifyThreads, 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap, 1, L.claims);
 }
 
 template <int PHASE, int V>
