@@ -43,6 +43,7 @@ extern "C" {
 #define THY_ERR_BUDGET 7       /* a scenario does not fit the server's HBM budget */
 #define THY_ERR_CANCELLED 8    /* a served request was cancelled */
 #define THY_ERR_TOO_LARGE 9    /* grid larger than an allocation-free entry point's fixed scratch */
+#define THY_ERR_TIMEOUT 10     /* a bounded wait on the device ran out (a staging copy did not land) */
 
 /* ------------------------------------------------------------------------
  * Raw problem: the contents of the problem .txt file and of its GRD and
@@ -229,6 +230,12 @@ int thy_session_tiling(const thy_session *s, thy_tiling *t);   /* tiling of the 
    and general units per step) is decided (*best set), 0 while tuning */
 int thy_session_tuned(const thy_session *s, thy_tiling *best);
 void thy_session_close(thy_session *s);
+/* Test hook for failure detection: with `what` = 1 the deep-water kernels
+   issue none of this session's staging copies, so their bounded waits
+   (about half a second) run out, the step stops and thy_session_steps
+   returns THY_ERR_TIMEOUT with the device context still usable; 0 turns it
+   off.  Nothing faults, traps or hangs. */
+int thy_session_inject(thy_session *s, int what);
 
 /* Autotuner of the warp tilings.  Every full chunk of a run (of any entry
    point) is timed as one sample of the tiling it ran with; the search, per

@@ -100,4 +100,5 @@ def test_abi_checks_tiling_arguments():
     assert L.thy_session_tune(None, 10, None) == thysea.THY_ERR_INVALID
     assert L.thy_session_tiling(None, None) == thysea.THY_ERR_INVALID
     assert L.thy_session_tuned(None, None) == thysea.THY_ERR_INVALID
+    assert L.thy_session_inject(None, 1) == thysea.THY_ERR_INVALID
     assert set(thysea.TILING_GROUPS) == {"deep1", "deep2", "general"}

@@ -63,8 +63,8 @@ struct ScenarioCtl {
     int nfaults;
     unsigned int dt_bits;      // atomicMin target (positive float bits)
     unsigned int tiles_done;   // phase-0 tiles finished (initial dt)
-    unsigned int errors;       // non-finite values seen
-    int pad_;
+    unsigned int errors;       // bit 0 non-finite values, bit 1 a staging copy did not land, bit 2 misaligned staging
+    int inject;                // test hook: bit 0 = the deep kernels issue none of this scenario's copies
     const double *fault_times; // nfaults fault times (s), sorted, device memory
     unsigned long long units_deep;   // work units stepped by the deep-water kernels (phase 2)
     unsigned long long units_dry;    // work units skipped as dry land (classifications)

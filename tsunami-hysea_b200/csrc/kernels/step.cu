@@ -428,10 +428,23 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
 }
 
 // at most 2^20 polls (each try_wait may suspend the thread for a while)
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// waits for the phase with this parity to complete; false after about half a
+// second (the copies it waits for did not land), so that no wait is endless
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
 {
-    for (int i = 0; i < (1 << 20); i++)
+    if (mbar_try_wait(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (int i = 0; i < (1 << 24); i++) {
         if (mbar_try_wait(bar, parity)) return true;
+        if (global_ns() - t0 > 500000000ull) return false;
+    }
     return false;
 }
 
@@ -635,6 +648,7 @@ struct DeepUnit {
     const ScenarioDev *s;
     int uidx, x0, yb, p;      // uidx: the unit's index in the scenario's unit grid
     bool run;
+    bool drop;                // test hook: issue no copy for it (its wait runs out)
 };
 static_assert(2 * sizeof(DeepUnit) + 16 <= kNextBytes, "claimed units' slots in shared memory");
 
@@ -653,6 +667,7 @@ __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ sc
     const ScenarioCtl *ctl = d.s->ctl;
     d.p = ctl->parity;
     d.run = *((volatile const int *)&ctl->status) == kRunning;
+    d.drop = (ctl->inject & 1) != 0;
     return d;
 }
 
@@ -733,7 +748,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
     uint32_t phase_bits = 0;     // bit b: parity of the next completion of bars[b]
     const TmaMap *acq = nullptr; // maps acquired by this CTA (producer)
     DeepUnit d = deep_unit(scen, work, lists, blockIdx.x);
-    if (threadIdx.x == PT && d.run) deep_issue<PHASE>(d, reinterpret_cast<float *>(dsm), &bars[0], acq);
+    if (threadIdx.x == PT && d.run && !d.drop) deep_issue<PHASE>(d, reinterpret_cast<float *>(dsm), &bars[0], acq);
     int buf = 0;
     // The first two waves take units blockIdx.x and blockIdx.x + gridDim.x;
     // after that each CTA claims its units from the counter (2 gridDim.x,
@@ -754,7 +769,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 if (un < nunits) {
                     const DeepUnit dn = deep_unit(scen, work, lists, un);
                     s_unit[buf ^ 1] = dn;
-                    if (dn.run)
+                    if (dn.run && !dn.drop)
                         deep_issue<PHASE>(dn, reinterpret_cast<float *>(dsm + (buf ^ 1) * SB), &bars[buf ^ 1], acq);
                     pending = 2 * (int)gridDim.x + atomicAdd(claim, 1);
                 }
@@ -918,8 +933,8 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
             // buffers' copies one more bounded wait so none is still writing; stop
             if (threadIdx.x == PT) {
                 atomicOr(&d.s->ctl->errors, 2u);
-                mbar_wait_bounded(&bars[buf], ((phase_bits >> buf) & 1u) ^ 1u);
-                if (s_next[buf ^ 1] < nunits && s_unit[buf ^ 1].run)
+                if (!d.drop) mbar_wait_bounded(&bars[buf], ((phase_bits >> buf) & 1u) ^ 1u);
+                if (s_next[buf ^ 1] < nunits && s_unit[buf ^ 1].run && !s_unit[buf ^ 1].drop)
                     mbar_wait_bounded(&bars[buf ^ 1], (phase_bits >> (buf ^ 1)) & 1u);
             }
             return;

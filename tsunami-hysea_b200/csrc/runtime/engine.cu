@@ -69,6 +69,13 @@ int ensure_device()
 
 int device_sm_count() { return g_sms[g_device] > 0 ? g_sms[g_device] : 148; }
 
+int failure_code(const ScenarioCtl &c)
+{
+    if (c.errors & 2u) return THY_ERR_TIMEOUT;
+    if (c.errors & 4u) return THY_ERR_CUDA;
+    return THY_ERR_NONFINITE;
+}
+
 // Page-locked host blocks reused across runs.  Pinning and unpinning are
 // driver calls that synchronise the device, and unpinning a block was seen to
 // stall a run's release for over half a second; freed blocks are kept by
@@ -1100,6 +1107,7 @@ extern "C" const char *thy_strerror(int code)
     case THY_ERR_CUDA: return last_error_text()[0] ? last_error_text() : "CUDA error";
     case THY_ERR_NO_DEVICE: return "there is no CUDA device";
     case THY_ERR_NONFINITE: return "the state or the time step became non-finite";
+    case THY_ERR_TIMEOUT: return "a bounded wait on the device ran out (a staging copy did not land)";
     case THY_ERR_BUDGET: return "scenario does not fit the HBM budget";
     case THY_ERR_CANCELLED: return "request cancelled";
     case THY_ERR_TOO_LARGE: return "grid exceeds the allocation-free entry point's maximum of 1048576 cells";
@@ -1167,7 +1175,7 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
         for (;;) {
             if (!(s.hctl.t < s.t_end)) break;
             if (s.max_steps >= 0 && s.hctl.step >= s.max_steps) break;
-            if (s.hctl.status == kFailed) { rc = THY_ERR_NONFINITE; goto out; }
+            if (s.hctl.status == kFailed) { rc = failure_code(s.hctl); goto out; }
             {
                 bool changed = false;
                 if ((rc = handle_events_ex(s, o, st, &changed))) goto out;
@@ -1179,7 +1187,7 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
             do {
                 if ((rc = b.run_chunk(true))) goto out;
             } while (s.hctl.status == kRunning);
-            if (s.hctl.status == kFailed) { rc = THY_ERR_NONFINITE; goto out; }
+            if (s.hctl.status == kFailed) { rc = failure_code(s.hctl); goto out; }
         }
         {
             auto t1 = std::chrono::steady_clock::now();
@@ -1268,7 +1276,7 @@ extern "C" int thy_session_steps(thy_session *S, long long steps, double *device
     }
     if (device_ms) *device_ms = S->b.device_ms - ms0;
     if (steps_done) *steps_done = s.hctl.step - start;
-    return s.hctl.status == kFailed ? THY_ERR_NONFINITE : THY_OK;
+    return s.hctl.status == kFailed ? failure_code(s.hctl) : THY_OK;
 }
 
 // Per-kernel device time: `steps` steps launched one kernel at a time with
@@ -1312,7 +1320,7 @@ extern "C" int thy_session_profile_launches(thy_session *S, long long steps, dou
     THY_CK(cudaStreamSynchronize(S->st));
     if (ms_per_launch)
         for (int j = 0; j < NL; j++) ms_per_launch[j] = t[j] / steps;
-    return s.hctl.status == kFailed ? THY_ERR_NONFINITE : THY_OK;
+    return s.hctl.status == kFailed ? failure_code(s.hctl) : THY_OK;
 }
 
 // Average device time of phase 1 and phase 2 (each the sum of its launches).
@@ -1349,6 +1357,13 @@ extern "C" int thy_session_fetch(thy_session *S, float *max_height, float *eta, 
 }
 
 extern "C" double thy_session_time(const thy_session *S) { return S ? S->s.hctl.t * S->s.Ts : 0.0; }
+
+extern "C" int thy_session_inject(thy_session *S, int what)
+{
+    if (!S || what < 0 || what > 1) return THY_ERR_INVALID;
+    S->s.hctl.inject = what;
+    return S->s.upload_ctl(S->st);
+}
 
 extern "C" int thy_session_tune(thy_session *S, long long max_steps, long long *steps_done)
 {

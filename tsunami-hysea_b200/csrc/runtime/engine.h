@@ -149,6 +149,8 @@ struct Batch {
 
 int ensure_device();
 int device_sm_count();
+// the THY_ERR_* code of a scenario the controller stopped as failed
+int failure_code(const ScenarioCtl &c);
 // page-locked host blocks, reused across runs (engine.cu)
 cudaError_t pinned_alloc(void **p, size_t bytes);
 void pinned_free(void *p);

@@ -226,7 +226,7 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             continue;
         }
         if (s.hctl.status == kFailed) {
-            complete(S, i, THY_ERR_NONFINITE);
+            complete(S, i, failure_code(s.hctl));
             continue;
         }
         const bool ended = !(s.hctl.t < s.t_end) || (s.max_steps >= 0 && s.hctl.step >= s.max_steps);
@@ -299,7 +299,7 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             Active *a = S->slots[i];
             if (!a) continue;
             const DevScenario &s = *a->s;
-            if (s.hctl.status == kFailed) complete(S, i, THY_ERR_NONFINITE);
+            if (s.hctl.status == kFailed) complete(S, i, failure_code(s.hctl));
             else if (!(s.hctl.t < s.t_end) || (s.max_steps >= 0 && s.hctl.step >= s.max_steps))
                 complete(S, i, THY_OK);
         }

@@ -21,7 +21,7 @@ from . import _ffi, synth  # noqa: F401
 
 THY_OK = 0
 THY_ERR_GPU_MEMORY, THY_ERR_HOST, THY_ERR_INVALID, THY_ERR_CUDA, THY_ERR_NO_DEVICE = 1, 2, 3, 4, 5
-THY_ERR_NONFINITE, THY_ERR_BUDGET, THY_ERR_CANCELLED, THY_ERR_TOO_LARGE = 6, 7, 8, 9
+THY_ERR_NONFINITE, THY_ERR_BUDGET, THY_ERR_CANCELLED, THY_ERR_TOO_LARGE, THY_ERR_TIMEOUT = 6, 7, 8, 9, 10
 
 
 class ThyError(RuntimeError):
@@ -267,6 +267,12 @@ class Session:
         k = ctypes.c_longlong()
         _check(_ffi.lib().thy_session_tune(self._h, max_steps, ctypes.byref(k)), "thy_session_tune")
         return k.value
+
+    def inject(self, what: int):
+        """Test hook (thy_session_inject): 1 = the deep-water kernels issue
+        none of this session's staging copies, so their bounded waits run out
+        and the next steps fail with THY_ERR_TIMEOUT; 0 = off."""
+        _check(_ffi.lib().thy_session_inject(self._h, what), "thy_session_inject")
 
     def tuned(self):
         """(decided, (deep1, deep2, general)) for the session's current work"""

@@ -132,6 +132,7 @@ SIGNATURES = {
                            ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
     "thy_session_close": ([ctypes.c_void_p], None),
     "thy_session_tune": ([ctypes.c_void_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)], ctypes.c_int),
+    "thy_session_inject": ([ctypes.c_void_p, ctypes.c_int], ctypes.c_int),
     "thy_session_tiling": ([ctypes.c_void_p, ctypes.POINTER(Tiling)], ctypes.c_int),
     "thy_tiling_force": ([ctypes.POINTER(Tiling)], ctypes.c_int),
     "thy_tiling_tuned": ([ctypes.c_double, ctypes.c_double, ctypes.POINTER(Tiling)], ctypes.c_int),
