@@ -25,15 +25,17 @@ struct Tiling {
     bool operator==(const Tiling &o) const { return deep1 == o.deep1 && deep2 == o.deep2 && general == o.general; }
     bool operator!=(const Tiling &o) const { return !(*this == o); }
 };
-// row groups per unit: deep phase 1 {3, 2, 4}, deep phase 2 {2, 1, 3}, general {2, 1, 4}
+// compute warps per CTA = 4 x deep_ng: deep phase 1 {3, 2, 4} (4 column strips
+// x that many row groups), deep phase 2 {2, 1, 4} (2 column strips of column
+// pairs x twice that many row groups); general {2, 1, 4} row groups
 __host__ __device__ constexpr int deep_ng(int phase, int v)
 {
-    return phase == 1 ? (v == 0 ? 3 : v == 1 ? 2 : 4) : (v == 0 ? 2 : v == 1 ? 1 : 3);
+    return phase == 1 ? (v == 0 ? 3 : v == 1 ? 2 : 4) : (v == 0 ? 2 : v == 1 ? 1 : 4);
 }
 // resident CTAs per SM the deep kernels are compiled for: phase 1 is held to
-// two by its staging buffers; phase 2 runs three unless 12 warps a CTA need
-// more registers than three CTAs leave
-__host__ __device__ constexpr int deep_minb(int phase, int v) { return phase == 1 ? 2 : (deep_ng(2, v) == 3 ? 2 : 3); }
+// two by its staging buffers; phase 2 (its lanes hold two columns) two, three
+// or one as its registers allow
+__host__ __device__ constexpr int deep_minb(int phase, int v) { return phase == 1 ? 2 : (v == 0 ? 2 : v == 1 ? 3 : 1); }
 __host__ __device__ constexpr int general_ng(int v) { return v == 0 ? 2 : v == 1 ? 1 : 4; }
 
 // step.cu

@@ -618,6 +618,101 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
     }
 }
 
+// ---------------------------------------------------------------------------
+// Deep phase 2 in pairs: a lane steps two adjacent columns, and the 2s
+// momentum fluxes, y edges and updates of the pair run in packed FP32x2
+// arithmetic (two lanes of FP32 per instruction, explicit round-to-nearest,
+// so no compiler contraction changes a result between code copies).  The
+// formulas are those of momentum_2s_x / momentum_2s_y.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, make_float2(-b.x, -b.y)); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 bc2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b)
+{
+    return make_float2(px ? a.x : b.x, py ? a.y : b.y);
+}
+__device__ __forceinline__ float2 rcp_depth2(float2 h) { return make_float2(rcp_depth(h.x), rcp_depth(h.y)); }
+__device__ __forceinline__ float2 sqrt2(float2 h) { return make_float2(sqrtf(h.x), sqrtf(h.y)); }
+
+// two cells of a staged row (columns i, i + 1; i even)
+struct Cell2 {
+    float2 h, e, D, qx, qy;
+};
+__device__ __forceinline__ Cell2 staged_cell2(const float *st, int i)
+{
+    Cell2 c;
+    c.e = *reinterpret_cast<const float2 *>(st + i);
+    c.D = *reinterpret_cast<const float2 *>(st + SPLANE + i);
+    c.qx = *reinterpret_cast<const float2 *>(st + 2 * SPLANE + i);
+    c.qy = *reinterpret_cast<const float2 *>(st + 3 * SPLANE + i);
+    c.h = add2(c.e, c.D);
+    return c;
+}
+
+struct MomFlux2 {
+    float2 m_x, m_y, p_x, p_y, lam;
+};
+struct Contrib2 {
+    float2 a, b, lam;
+};
+
+// momentum_2s_x for two edges at once
+__device__ __forceinline__ void momentum_2s_x2(MomFlux2 &r, float2 h0, float2 h1, float2 rh0, float2 rh1, float2 s0,
+                                               float2 s1, float2 u0, float2 u1, float2 v0, float2 v1, float2 jump,
+                                               const XRowK &k)
+{
+    const float2 hij = mul2(bc2(0.5f), add2(h0, h1));
+    const float2 u0n = mul2(u0, rh0), u1n = mul2(u1, rh1);
+    const float2 num = fma2(s0, u0n, mul2(s1, u1n));
+    const float2 den = add2(add2(s0, s1), bc2(kEps));
+    const float2 uijn = make_float2(__fdividef(num.x, den.x), __fdividef(num.y, den.y));
+    const float2 maxa = add2(make_float2(fabsf(uijn.x), fabsf(uijn.y)), sqrt2(hij));
+    const bool nx_ = uijn.x < 0.f, ny_ = uijn.y < 0.f;
+    const float2 un = sel2(nx_, ny_, u1n, u0n), uu = sel2(nx_, ny_, u1, u0), vv = sel2(nx_, ny_, v1, v0);
+    const float2 il = bc2(k.ilcos);
+    const float2 mx0 = mul2(mul2(un, uu), il);
+    const float2 mx = fma2(mul2(hij, jump), il, mx0);
+    const float2 my = mul2(mul2(un, vv), il);
+    const float2 des = mul2(mul2(bc2(k.kdes), mul2(maxa, maxa)), sub2(u1, u0));
+    r.m_x = sub2(mx, des);
+    r.m_y = my;
+    r.p_x = sub2(des, mx0);
+    r.p_y = neg2(my);
+    r.lam = mul2(il, maxa);
+}
+
+// momentum_2s_y for two edges at once (one row pair: the constants are shared)
+__device__ __forceinline__ void momentum_2s_y2(MomFlux2 &r, float2 h0, float2 h1, float2 rh0, float2 rh1, float2 s0,
+                                               float2 s1, float2 u0, float2 u1, float2 v0, float2 v1, float2 jump,
+                                               const YRowK &k)
+{
+    const float2 hij = mul2(bc2(0.5f), add2(h0, h1));
+    const float2 u0n = mul2(u0, rh0), u1n = mul2(u1, rh1);
+    const float2 num = fma2(s0, u0n, mul2(s1, u1n));
+    const float2 den = add2(add2(s0, s1), bc2(kEps));
+    const float2 uijn = make_float2(__fdividef(num.x, den.x), __fdividef(num.y, den.y));
+    const float2 maxa = add2(make_float2(fabsf(uijn.x), fabsf(uijn.y)), sqrt2(hij));
+    const float2 deta = fma2(neg2(mul2(uijn, uijn)), bc2(k.cdiff), mul2(bc2(k.cmid), jump));
+    const bool nx_ = uijn.x < 0.f, ny_ = uijn.y < 0.f;
+    const float2 un = sel2(nx_, ny_, u1n, u0n), uu = sel2(nx_, ny_, u1, u0), vv = sel2(nx_, ny_, v1, v0);
+    const float2 len = bc2(k.len);
+    const float2 fym0 = mul2(mul2(un, uu), len);
+    // upwind from below: fyp = -fym0, fym = fym0 cos1/cos0; from above: fyp = -fym0 cos0/cos1, fym = fym0
+    const float2 fyp = mul2(neg2(fym0), sel2(nx_, ny_, bc2(1.f), bc2(k.c01)));
+    const float2 fym = fma2(mul2(hij, deta), bc2(k.li0), mul2(fym0, sel2(nx_, ny_, bc2(k.c10), bc2(1.f))));
+    const float2 fxm = mul2(mul2(un, vv), len);
+    const float2 m2 = mul2(mul2(maxa, maxa), fma2(u1, bc2(k.cos1), neg2(mul2(u0, bc2(k.cos0)))));
+    r.m_x = fxm;
+    r.m_y = fma2(bc2(-k.kdes0), m2, fym);
+    r.p_x = neg2(fxm);
+    r.p_y = fma2(bc2(k.kdes1), m2, fyp);
+    r.lam = mul2(len, maxa);
+}
+
 // y edge between rows gy-1 (a, row metrics ra) and gy (b, rb) of a deep tile;
 // phase 2 also takes 1/h and sqrt(h) of both cells, and the edge's constants
 // from rb
@@ -641,6 +736,22 @@ __device__ __forceinline__ void y_edge_deep(const ScenarioDev &s, const Cell &a,
         lo = {-f.m_x, -f.m_y, f.lam};
         hi = {-f.p_x, -f.p_y, f.lam};
     }
+}
+
+// y edge of phase 2 between rows a (metrics ra) and b (rb) for two columns
+__device__ __forceinline__ void y_edge_deep2(const Cell2 &a, const Cell2 &b, float2 rha, float2 sha, float2 rhb,
+                                             float2 shb, const DeepRow &ra, const DeepRow &rb, Contrib2 &lo,
+                                             Contrib2 &hi)
+{
+    YRowK k;
+    k.len = rb.y0.x; k.cmid = rb.y0.y; k.cdiff = rb.y0.z; k.c10 = rb.y0.w;
+    k.c01 = rb.y1.x; k.li0 = rb.y1.y; k.kdes0 = rb.y1.z; k.kdes1 = rb.y1.w;
+    k.cos0 = ra.m.x; k.cos1 = rb.m.x;
+    const float2 jump = make_float2(surface_jump(a.e.x, b.e.x, a.D.x, b.D.x), surface_jump(a.e.y, b.e.y, a.D.y, b.D.y));
+    MomFlux2 f;
+    momentum_2s_y2(f, a.h, b.h, rha, rhb, sha, shb, a.qy, b.qy, a.qx, b.qx, jump, k);
+    lo = {neg2(f.m_x), neg2(f.m_y), f.lam};
+    hi = {neg2(f.p_x), neg2(f.p_y), f.lam};
 }
 
 // A deep work unit: unit code u = 2 * (work-list index) + half.
@@ -799,6 +910,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
             // the compute warps only: the row constants are written, every copy checked
             asm volatile("bar.sync 1, %0;" ::"r"(PT) : "memory");
             if (!s_err) {
+              if constexpr (PHASE == 1) {
                 // phase 1: the row metrics as staged (row t of the window at t + 1)
                 const float4 *rowm =
                     reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE)) + 1;
@@ -922,6 +1034,80 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     red[warp] = (PHASE == 1) ? local_min : local_max;
                     if (PHASE == 1) red[NW + warp] = local_max;
                 }
+              } else {
+                // phase 2 in pairs: two column strips of 56 cells; lane l
+                // steps staged columns sc0 and sc0 + 1 (lanes 1..28 are cells,
+                // lanes 0 and 29 the halo, lanes 30 and 31 repeat lane 29)
+                constexpr int NG2 = 2 * NG;
+                const int strip2 = warp & 1, group2 = warp >> 1;
+                const int prow0 = kHalfRows * group2 / NG2, pnrows = kHalfRows * (group2 + 1) / NG2 - prow0;
+                const int sc0 = strip2 * 56 + 2 + 2 * min(lane, 29);
+                const bool out_lane = (lane >= 1) && (lane <= 28);
+                const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
+                const int pitch = s.pitch;
+                const int r_first = prow0 + 1;                    // staged row of this warp's first output row
+                float local_max = -FLT_MAX;                        // max of lam / (2 cfl area)
+                int i = r_first * kStageW + sc0;
+                Cell2 c = staged_cell2(stage, i);
+                float2 rh_c = rcp_depth2(c.h), sh_c = sqrt2(c.h);
+                DeepRow rc = rows[r_first];
+                Contrib2 top;
+                {
+                    const Cell2 a = staged_cell2(stage, i - kStageW);
+                    Contrib2 dummy;
+                    y_edge_deep2(a, c, rcp_depth2(a.h), sqrt2(a.h), rh_c, sh_c, rows[r_first - 1], rc, dummy, top);
+                }
+                float *out0 = s.qx[p ^ 1], *out1 = s.qy[p ^ 1];
+                int off = (yb + r_first - 1) * pitch + x0 - 4 + sc0;
+                float2 fin = make_float2(0.f, 0.f);   // running sum: non-finite iff a new value is
+                for (int k = 0; k < pnrows; k++, i += kStageW, off += pitch) {
+                    const DeepRow rn = rows[r_first + k + 1];
+                    const Cell2 n = staged_cell2(stage, i + kStageW);
+                    const float2 rh_n = rcp_depth2(n.h), sh_n = sqrt2(n.h);
+                    // y edges below this row
+                    Contrib2 below, next_top;
+                    y_edge_deep2(c, n, rh_c, sh_c, rh_n, sh_n, rc, rn, below, next_top);
+                    // x edges left of column sc0 (its left neighbour from shared
+                    // memory, 1/h and sqrt h from lane l-1) and between sc0 and sc0 + 1
+                    const float le = stage[i - 1], lD = stage[SPLANE + i - 1];
+                    const float lqx = stage[2 * SPLANE + i - 1], lqy = stage[3 * SPLANE + i - 1];
+                    const float rhL = shup(rh_c.y, 1), shL = shup(sh_c.y, 1);
+                    const float2 jump =
+                        make_float2(surface_jump(le, c.e.x, lD, c.D.x), surface_jump(c.e.x, c.e.y, c.D.x, c.D.y));
+                    MomFlux2 f;
+                    momentum_2s_x2(f, make_float2(le + lD, c.h.x), c.h, make_float2(rhL, rh_c.x), rh_c,
+                                   make_float2(shL, sh_c.x), sh_c, make_float2(lqx, c.qx.x), c.qx,
+                                   make_float2(lqy, c.qy.x), c.qy, jump, XRowK{rc.m.y, rc.kdx});
+                    // column sc0: right cell of the left edge, left cell of the
+                    // middle edge; column sc0 + 1: right cell of the middle edge,
+                    // left cell of lane l+1's left edge
+                    const Contrib2 xr = {neg2(f.p_x), neg2(f.p_y), f.lam};
+                    const Contrib2 xrr = {make_float2(-f.m_x.y, -shdn(f.m_x.x, 1)),
+                                          make_float2(-f.m_y.y, -shdn(f.m_y.x, 1)),
+                                          make_float2(f.lam.y, shdn(f.lam.x, 1))};
+                    // momentum update; the dt bound as in the scalar path
+                    const float2 lam = add2(add2(add2(xr.lam, xrr.lam), top.lam), below.lam);
+                    const float2 w = mul2(lam, bc2(rc.kcfl));
+                    const float wm = fmaxf(lam.x < kEps ? 0.f : w.x, lam.y < kEps ? 0.f : w.y);
+                    if (out_lane) local_max = fmaxf(local_max, wm);
+                    const float2 val = bc2(rc.dtA);
+                    const float2 qx = fma2(val, add2(add2(add2(xr.a, xrr.a), top.a), below.a), c.qx);
+                    const float2 qy = fma2(val, add2(add2(add2(xr.b, xrr.b), top.b), below.b), c.qy);
+                    if (out_lane) {
+                        fin = add2(fin, add2(qx, qy));
+                        *reinterpret_cast<float2 *>(out0 + off) = qx;
+                        *reinterpret_cast<float2 *>(out1 + off) = qy;
+                    }
+                    top = next_top;
+                    rc = rn;
+                    c = n;
+                    rh_c = rh_n;
+                    sh_c = sh_n;
+                }
+                if (!isfinite(fin.x) || !isfinite(fin.y)) atomicOr(&ctl->errors, 1u);
+                for (int o = 16; o > 0; o >>= 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
+                if (lane == 0) red[warp] = local_max;
+              }
             }
         }
         if (d.run) phase_bits ^= 1u << buf;
