@@ -1038,9 +1038,10 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 // phase 2 in pairs: two column strips of 56 cells; lane l
                 // steps staged columns sc0 and sc0 + 1 (lanes 1..28 are cells,
                 // lanes 0 and 29 the halo, lanes 30 and 31 repeat lane 29)
-                constexpr int NG2 = 2 * NG;
+                constexpr int NG2 = 2 * NG, PROWS = kHalfRows / NG2;   // row groups, rows per warp
+                static_assert(kHalfRows % NG2 == 0, "phase-2 row groups of equal height");
                 const int strip2 = warp & 1, group2 = warp >> 1;
-                const int prow0 = kHalfRows * group2 / NG2, pnrows = kHalfRows * (group2 + 1) / NG2 - prow0;
+                const int prow0 = PROWS * group2;
                 const int sc0 = strip2 * 56 + 2 + 2 * min(lane, 29);
                 const bool out_lane = (lane >= 1) && (lane <= 28);
                 const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
@@ -1060,7 +1061,11 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 float *out0 = s.qx[p ^ 1], *out1 = s.qy[p ^ 1];
                 int off = (yb + r_first - 1) * pitch + x0 - 4 + sc0;
                 float2 fin = make_float2(0.f, 0.f);   // running sum: non-finite iff a new value is
-                for (int k = 0; k < pnrows; k++, i += kStageW, off += pitch) {
+                // two rows an iteration, so that the row window is renamed
+                // rather than copied (every operation here is explicitly
+                // rounded: the copies compute alike)
+#pragma unroll 2
+                for (int k = 0; k < PROWS; k++, i += kStageW, off += pitch) {
                     const DeepRow rn = rows[r_first + k + 1];
                     const Cell2 n = staged_cell2(stage, i + kStageW);
                     const float2 rh_n = rcp_depth2(n.h), sh_n = sqrt2(n.h);
