@@ -489,7 +489,7 @@ static_assert((SPLANE * 4) % 128 == 0 && (DPLANE * 4) % 128 == 0, "staged planes
 // and descriptor, one slot per buffer parity) and the error flag, the staged
 // row metrics of the current unit and the reduction scratch (one set per
 // buffer parity).
-constexpr size_t kNextBytes = 80;   // s_next[2], s_err, pad, s_unit[2]
+constexpr size_t kNextBytes = 16 + 2 * 112;   // s_next[2], s_err, pad, s_unit[2]
 // A phase-1 staging buffer also receives the unit's packed row metrics, rows
 // yb-2 .. yb+16 (a deep unit lies at least two rows inside the grid), copied
 // with the planes so that they arrive one unit ahead too; phase 2 derives its
@@ -755,14 +755,24 @@ __device__ __forceinline__ void y_edge_deep2(const Cell2 &a, const Cell2 &b, flo
 }
 
 // A deep work unit: unit code u = 2 * (work-list index) + half.
+// A deep unit and what its compute warps read of its scenario (read by the
+// producer when it claims the unit, so that the compute warps start the unit
+// from shared memory): dt, time and parity are fixed during a launch.
 struct DeepUnit {
     const ScenarioDev *s;
+    ScenarioCtl *ctl;
+    float *out0, *out1;       // phase 1: eta at the new parity; phase 2: qx, qy at the new parity
+    float *eta_max, *arr;     // phase 1 diagnostics
+    const float4 *rowpack;    // phase 2 row metrics
     int uidx, x0, yb, p;      // uidx: the unit's index in the scenario's unit grid
+    int pitch;
+    float dt, t_sec, eps_h, dif_at, cfl, cvis;
     bool run;
     bool drop;                // test hook: issue no copy for it (its wait runs out)
 };
 static_assert(2 * sizeof(DeepUnit) + 16 <= kNextBytes, "claimed units' slots in shared memory");
 
+template <int PHASE>
 __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
                                               const int *__restrict__ lists, int i)
 {
@@ -775,10 +785,24 @@ __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ sc
     d.uidx = uy * d.s->tiles_x + tx;
     d.x0 = tx * kTileX;
     d.yb = uy * kHalfRows;
-    const ScenarioCtl *ctl = d.s->ctl;
+    const ScenarioDev &s = *d.s;
+    ScenarioCtl *ctl = s.ctl;
+    d.ctl = ctl;
     d.p = ctl->parity;
     d.run = *((volatile const int *)&ctl->status) == kRunning;
     d.drop = (ctl->inject & 1) != 0;
+    d.pitch = s.pitch;
+    d.dt = (float)ctl->dt;
+    d.t_sec = (PHASE == 1) ? (float)(ctl->t * ctl->T) : 0.f;
+    d.eps_h = s.eps_h;
+    d.dif_at = s.dif_at;
+    d.cfl = s.cfl;
+    d.cvis = s.cvis;
+    d.out0 = (PHASE == 1) ? s.eta[d.p ^ 1] : s.qx[d.p ^ 1];
+    d.out1 = s.qy[d.p ^ 1];
+    d.eta_max = s.eta_max;
+    d.arr = s.arr;
+    d.rowpack = s.rowpack;
     return d;
 }
 
@@ -858,7 +882,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
     __syncthreads();
     uint32_t phase_bits = 0;     // bit b: parity of the next completion of bars[b]
     const TmaMap *acq = nullptr; // maps acquired by this CTA (producer)
-    DeepUnit d = deep_unit(scen, work, lists, blockIdx.x);
+    DeepUnit d = deep_unit<PHASE>(scen, work, lists, blockIdx.x);
     if (threadIdx.x == PT && d.run && !d.drop) deep_issue<PHASE>(d, reinterpret_cast<float *>(dsm), &bars[0], acq);
     int buf = 0;
     // The first two waves take units blockIdx.x and blockIdx.x + gridDim.x;
@@ -878,7 +902,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 const int un = pending;
                 s_next[buf ^ 1] = un;
                 if (un < nunits) {
-                    const DeepUnit dn = deep_unit(scen, work, lists, un);
+                    const DeepUnit dn = deep_unit<PHASE>(scen, work, lists, un);
                     s_unit[buf ^ 1] = dn;
                     if (dn.run && !dn.drop)
                         deep_issue<PHASE>(dn, reinterpret_cast<float *>(dsm + (buf ^ 1) * SB), &bars[buf ^ 1], acq);
@@ -887,21 +911,21 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
             }
         } else if (d.run) {
             const ScenarioDev &s = *d.s;
-            ScenarioCtl *ctl = s.ctl;
-            const int x0 = d.x0, yb = d.yb, p = d.p;
-            const float dt = (float)ctl->dt;
+            ScenarioCtl *ctl = d.ctl;
+            const int x0 = d.x0, yb = d.yb;
+            const float dt = d.dt;
             if (PHASE == 2 && threadIdx.x < kStageRows) {
                 // row constants of the window with the unit's dt folded in,
                 // while the copies are in flight; staged row t is grid row
                 // yb - 1 + t
                 DeepRow r;
-                r.m = __ldg(s.rowpack + yb - 1 + threadIdx.x);
-                const float4 a = __ldg(s.rowpack + yb - 2 + threadIdx.x);   // the row above
+                r.m = __ldg(d.rowpack + yb - 1 + threadIdx.x);
+                const float4 a = __ldg(d.rowpack + yb - 2 + threadIdx.x);   // the row above
                 r.icos = __frcp_rn(r.m.x);
                 r.dtA = __fdividef(dt, r.m.z);
-                r.kcfl = 1.f / (2.f * s.cfl * r.m.z);
-                r.kdx = make_xrow(r.m.y, r.m.z + r.m.z, dt, s.cvis).kdes;
-                const YRowK k = make_yrow(a.x, r.m.x, __frcp_rn(a.x), r.icos, r.m.w, a.z + r.m.z, dt, s.cvis);
+                r.kcfl = 1.f / (2.f * d.cfl * r.m.z);
+                r.kdx = make_xrow(r.m.y, r.m.z + r.m.z, dt, d.cvis).kdes;
+                const YRowK k = make_yrow(a.x, r.m.x, __frcp_rn(a.x), r.icos, r.m.w, a.z + r.m.z, dt, d.cvis);
                 r.y0 = make_float4(k.len, k.cmid, k.cdiff, k.c10);
                 r.y1 = make_float4(k.c01, k.li0, k.kdes0, k.kdes1);
                 rows[threadIdx.x] = r;
@@ -921,8 +945,8 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     return r;
                 };
                 const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
-                const float t_sec = (float)(ctl->t * ctl->T);
-                const int pitch = s.pitch;
+                const float t_sec = d.t_sec;
+                const int pitch = d.pitch;
                 const int r_first = row0 + 1;                           // staged row of this warp's first output row
                 const int sc = strip * 28 + 2 + lane;                   // staged column of this lane
                 const int gx = x0 - 4 + sc;                             // grid column
@@ -950,8 +974,8 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     Contrib dummy;
                     y_edge_deep<PHASE>(s, a, c, rh_a, sh_a, rh_c, sh_c, row(r_first - 1), rc, dt, dummy, top);
                 }
-                float *out0 = (PHASE == 1) ? s.eta[p ^ 1] : s.qx[p ^ 1];
-                float *out1 = s.qy[p ^ 1];
+                float *out0 = d.out0;
+                float *out1 = d.out1;
                 int off = (yb + r_first - 1) * pitch + gx;
                 // running sum of the cells' new values: non-finite iff one of them is
                 float fin = 0.f;
@@ -994,8 +1018,8 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                         // diagnostics of the state the step starts from (src/GPU/Metrics.cu:23-77)
                         const float *dg = stage + 4 * SPLANE + (r_first - 1 + k) * kTileX + dcol;
                         const float em = dg[0], ar = dg[DPLANE], ei = dg[2 * DPLANE];
-                        if (c.e > em && c.h > s.eps_h) s.eta_max[off] = c.e;
-                        if (ar < 0.f && fabsf(c.e - ei) > s.dif_at) s.arr[off] = t_sec;
+                        if (c.e > em && c.h > d.eps_h) d.eta_max[off] = c.e;
+                        if (ar < 0.f && fabsf(c.e - ei) > d.dif_at) d.arr[off] = t_sec;
                         // mass update (src/GPU/Volumen_kernel.cu:111-157)
                         const float acc = ((xr.a + xrr.a) + top.a) + below.a;
                         float eta = c.e + __fdividef(dt, area) * acc;
@@ -1045,7 +1069,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 const int sc0 = strip2 * 56 + 2 + 2 * min(lane, 29);
                 const bool out_lane = (lane >= 1) && (lane <= 28);
                 const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
-                const int pitch = s.pitch;
+                const int pitch = d.pitch;
                 const int r_first = prow0 + 1;                    // staged row of this warp's first output row
                 float local_max = -FLT_MAX;                        // max of lam / (2 cfl area)
                 int i = r_first * kStageW + sc0;
@@ -1058,7 +1082,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     Contrib2 dummy;
                     y_edge_deep2(a, c, rcp_depth2(a.h), sqrt2(a.h), rh_c, sh_c, rows[r_first - 1], rc, dummy, top);
                 }
-                float *out0 = s.qx[p ^ 1], *out1 = s.qy[p ^ 1];
+                float *out0 = d.out0, *out1 = d.out1;
                 int off = (yb + r_first - 1) * pitch + x0 - 4 + sc0;
                 float2 fin = make_float2(0.f, 0.f);   // running sum: non-finite iff a new value is
                 // two rows an iteration, so that the row window is renamed
@@ -1134,7 +1158,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
         const DeepUnit dn = s_unit[buf ^ 1];   // valid when un < nunits
         if (d.run && threadIdx.x == PT) {
             const ScenarioDev &s = *d.s;
-            ScenarioCtl *ctl = s.ctl;
+            ScenarioCtl *ctl = d.ctl;
             float m = red[0];
             for (int k = 1; k < NW; k++) m = (PHASE == 1) ? fminf(m, red[k]) : fmaxf(m, red[k]);
             // phase 2: the unit's dt bound from its largest lam / (2 cfl area),
