@@ -221,8 +221,9 @@ __device__ __forceinline__ bool all_deep(const Edge &e, float hpos)
 // Edges whose four stencil cells are all deeper than hpos and which lie at
 // least two cells from a boundary: the 2s blend weight is exactly 1, so the
 // flux is the 2s flux alone (the WAF part, the wet/dry tests and the limiter
-// drop out).  The general functions below and the deep-water kernels both
-// call these, so both paths produce the same numbers.
+// drop out).  The general functions below and deep phase 1 call these; deep
+// phase 2 evaluates the same formulas two edges at a time in packed FP32x2
+// arithmetic (step.cu), which can round its last bit differently.
 // ---------------------------------------------------------------------------
 
 // x edge: F = q0 len, outflow-limited (src/GPU/Arista_kernel.cu:118-219, alfa = 1)
@@ -254,7 +255,7 @@ __device__ __forceinline__ float rcp_depth(float h) { return __fdividef(1.f, h);
 // Constants of the 2s momentum flux that depend only on the edge's row (its
 // metrics), the step's dt and the scenario's viscosity: the deep-water kernels
 // form them once per row of a unit, the general kernel per edge, with the same
-// expressions, so both paths give the same fluxes.
+// expressions.
 struct XRowK {
     float ilcos;   // len / cos of the row
     float kdes;    // cd * val * ilcos, val = 2 ilcos dt / (area0 + area1), cd = (1 - cvis) / 2

@@ -724,8 +724,8 @@ __device__ __forceinline__ void y_edge_deep(const ScenarioDev &s, const Cell &a,
     const float cos0 = ra.m.x, cos1 = rb.m.x;
     if (PHASE == 1) {
         const float F = mass_2s_y(a.qy, rb.m.w, cos0, cos1, a.h, b.h, dt, ra.m.z, rb.m.z);
-        lo = {-F / cos0, 0.f, 0.f};
-        hi = {F / cos1, 0.f, 0.f};
+        lo = {-F * ra.icos, 0.f, 0.f};
+        hi = {F * rb.icos, 0.f, 0.f};
     } else {
         YRowK k;
         k.len = rb.y0.x; k.cmid = rb.y0.y; k.cdiff = rb.y0.z; k.c10 = rb.y0.w;
@@ -931,19 +931,21 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 rows[threadIdx.x] = r;
             }
             if (!mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u)) s_err = 1;
+            if (PHASE == 1 && threadIdx.x < kStageRows) {
+                // phase 1 row constants from the staged row metrics (row t of
+                // the window at t + 1): 1/cos for the y edges, dt/area
+                const float4 *raw = reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE));
+                DeepRow r;
+                r.m = raw[threadIdx.x + 1];
+                r.icos = __frcp_rn(r.m.x);
+                r.dtA = __fdividef(dt, r.m.z);
+                rows[threadIdx.x] = r;
+            }
             // the compute warps only: the row constants are written, every copy checked
             asm volatile("bar.sync 1, %0;" ::"r"(PT) : "memory");
             if (!s_err) {
               if constexpr (PHASE == 1) {
-                // phase 1: the row metrics as staged (row t of the window at t + 1)
-                const float4 *rowm =
-                    reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE)) + 1;
-                auto row = [&](int t) {
-                    if (PHASE == 2) return rows[t];
-                    DeepRow r;
-                    r.m = rowm[t];
-                    return r;
-                };
+                auto row = [&](int t) { return rows[t]; };
                 const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
                 const float t_sec = d.t_sec;
                 const int pitch = d.pitch;
@@ -1022,7 +1024,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                         if (ar < 0.f && fabsf(c.e - ei) > d.dif_at) d.arr[off] = t_sec;
                         // mass update (src/GPU/Volumen_kernel.cu:111-157)
                         const float acc = ((xr.a + xrr.a) + top.a) + below.a;
-                        float eta = c.e + __fdividef(dt, area) * acc;
+                        float eta = c.e + rc.dtA * acc;
                         if (!(eta + c.D > 0.f)) eta = -c.D;
                         fin += eta;
                         out0[off] = eta;
