@@ -289,8 +289,11 @@ __device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const UnitSum *_
     const int W = s.tiles_x;
     const UnitSum *c = sum + (size_t)uy * W + tx;
     const float hp = s.hpos;
-    return (c->all.x > hp) && (c[-1].R.x > hp) && (c[1].L.x > hp) && (c[-W].B.x > hp) && (c[W].T.x > hp) &&
-           (c[-W - 1].BR.x > hp) && (c[-W + 1].BL.x > hp) && (c[W - 1].TR.x > hp) && (c[W + 1].TL.x > hp);
+    // all nine loads first and no short-circuit, so that they are in flight
+    // together (a NaN, an unknown summary, fails its test as before)
+    const float v0 = c->all.x, v1 = c[-1].R.x, v2 = c[1].L.x, v3 = c[-W].B.x, v4 = c[W].T.x;
+    const float v5 = c[-W - 1].BR.x, v6 = c[-W + 1].BL.x, v7 = c[W - 1].TR.x, v8 = c[W + 1].TL.x;
+    return (v0 > hp) & (v1 > hp) & (v2 > hp) & (v3 > hp) & (v4 > hp) & (v5 > hp) & (v6 > hp) & (v7 > hp) & (v8 > hp);
 }
 
 // Outside the grid counts as dry (ghost cells copy the boundary cell), except
@@ -299,9 +302,12 @@ __device__ __forceinline__ bool unit_dry(const ScenarioDev &s, const UnitSum *__
 {
     const int ny_u = units_y(s), nx_u = s.tiles_x;
     bool dry = true;
+    // every neighbour's load issued without waiting for the previous test
+#pragma unroll
     for (int dy = -1; dy <= 1; dy++) {
         const int y = uy + dy;
         if (y < 0 || y >= ny_u) continue;
+#pragma unroll
         for (int dx = -1; dx <= 1; dx++) {
             int x = tx + dx;
             if (x < 0 || x >= nx_u) {
@@ -315,7 +321,7 @@ __device__ __forceinline__ bool unit_dry(const ScenarioDev &s, const UnitSum *__
                            : (dx == 0) ? (dy < 0 ? u.B : u.T)
                            : (dy < 0) ? (dx < 0 ? u.BR : u.BL)
                                       : (dx < 0 ? u.TR : u.TL);
-            dry = dry && (v.y <= 0.f);
+            dry &= (v.y <= 0.f);
         }
     }
     return dry;
