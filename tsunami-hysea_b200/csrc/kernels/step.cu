@@ -153,57 +153,66 @@ __device__ __forceinline__ float initial_speed(Edge &e, const ScenarioDev &s)
 //  src/GPU/Timestep.cu:35-68 dt truncation to fault times).
 __device__ void controller(const ScenarioDev &s)
 {
-    ScenarioCtl *c = s.ctl;
-    const float dmin = __uint_as_float(atomicOr(&c->dt_bits, 0u));
-    const unsigned errs = atomicOr(&c->errors, 0u);
-    c->t += c->dt;
+    // one thread per scenario, in its own launch after the phase-2 kernels:
+    // the control block is read once (plain loads see their atomics), updated
+    // in registers and the changed fields written back
+    ScenarioCtl *cp = s.ctl;
+    ScenarioCtl c = *cp;
+    const float dmin = __uint_as_float(c.dt_bits);
+    const unsigned errs = c.errors;
+    c.t += c.dt;
     double dt = (double)dmin;
     // truncation so that t lands on the next fault time
-    const int nf = c->nfaults;
-    const int f = c->fault_next;
-    const double *tf = c->fault_times;
-    if (!c->jumping) {
-        if (f < nf && (c->t + dt) * c->T > tf[f]) {
-            dt = tf[f] / c->T - c->t;
-            c->jumping = 1;
+    const int nf = c.nfaults;
+    const int f = c.fault_next;
+    const double *tf = c.fault_times;
+    if (!c.jumping) {
+        if (f < nf && (c.t + dt) * c.T > tf[f]) {
+            dt = tf[f] / c.T - c.t;
+            c.jumping = 1;
         }
     } else {
-        c->jumping = 0;
+        c.jumping = 0;
         if (f < nf) {
             int i = f + 1;
             while (i < nf && !(fabs(tf[i] - tf[f]) > 2.220446049250313e-16)) i++;
-            if (i < nf && (c->t + dt) * c->T > tf[i]) {
-                dt = tf[i] / c->T - c->t;
-                c->jumping = 1;
+            if (i < nf && (c.t + dt) * c.T > tf[i]) {
+                dt = tf[i] / c.T - c.t;
+                c.jumping = 1;
             }
         }
     }
-    c->dt = dt;
-    c->step += 1;
-    c->parity ^= 1;
-    c->dt_bits = 0x7f7fffffu;
-    c->tiles_done = 0u;
+    c.dt = dt;
+    c.step += 1;
+    c.parity ^= 1;
+    c.dt_bits = 0x7f7fffffu;
+    c.tiles_done = 0u;
     int ev = 0;
     if (errs || !(dmin > 0.f) || isnan(dmin)) {
-        c->status = kFailed;
-        return;
+        c.status = kFailed;
+    } else if (!(c.t < c.t_end)) {
+        c.status = kDone;
+    } else if (c.max_steps >= 0 && c.step >= c.max_steps) {
+        c.events = kEvStepBudget;
+        c.status = kDone;
+    } else {
+        if (f < nf && c.t * c.T >= tf[f]) ev |= kEvFault;
+        if (c.save_nc >= 0.0 && c.t >= c.next_nc) ev |= kEvSnapshot;
+        if (c.save_ts >= 0.0 && c.t >= c.next_ts) ev |= kEvSeries;
+        if (ev) {
+            c.events = ev;
+            c.status = kPaused;
+        }
     }
-    if (!(c->t < c->t_end)) {
-        c->status = kDone;
-        return;
-    }
-    if (c->max_steps >= 0 && c->step >= c->max_steps) {
-        c->events = kEvStepBudget;
-        c->status = kDone;
-        return;
-    }
-    if (f < nf && c->t * c->T >= tf[f]) ev |= kEvFault;
-    if (c->save_nc >= 0.0 && c->t >= c->next_nc) ev |= kEvSnapshot;
-    if (c->save_ts >= 0.0 && c->t >= c->next_ts) ev |= kEvSeries;
-    if (ev) {
-        c->events = ev;
-        c->status = kPaused;
-    }
+    cp->t = c.t;
+    cp->dt = c.dt;
+    cp->step = c.step;
+    cp->parity = c.parity;
+    cp->jumping = c.jumping;
+    cp->dt_bits = c.dt_bits;
+    cp->tiles_done = c.tiles_done;
+    cp->events = c.events;
+    cp->status = c.status;
 }
 
 // Edge between rows gy-1 (a) and gy (b) of this lane's column, stencil rows
