@@ -96,6 +96,7 @@ struct UnitSum {
 struct ScenarioDev {
     int nx, ny, pitch;
     int tiles_x, tiles_y, ntiles;
+    int x_org;   // grid column of tile 0's first column (tile_origin: 0 or -4 .. -108)
     int periodic;
     float b_up, b_low, b_left, b_right;
     int sp_up, sp_low, sp_left, sp_right;
@@ -108,8 +109,8 @@ struct ScenarioDev {
     float *eta_max;
     float *arr;
     float *eta_ini;
-    // per work unit (half tile of kTileX x kHalfRows cells; unit (tx, uy) at
-    // uy * tiles_x + tx): depth summary of the state phase 1 produces (index
+    // per work unit (half tile of kTileX x kHalfRows cells from column
+    // x_org + tx kTileX; unit (tx, uy) at uy * tiles_x + tx): depth summary of the state phase 1 produces (index
     // parity^1); NaN = unknown
     UnitSum *usum[2];
     // per unit: consecutive classifications that found its 3 x 3 unit

@@ -12,6 +12,35 @@ constexpr int kStepThreads = 128;           // 4 warps = 4 column strips per til
 constexpr int kTileX = 28 * (kStepThreads / 32);   // tile width: 28 output columns per warp
 constexpr int kTileY = 32;                  // tile height: rows one warp marches through
 
+// Grid column where tile 0 starts: 0 or a negative multiple of 4 above
+// -kTileX (tile 0 then holds its last 4 .. 108 columns), so that the deep
+// kernels' boxes at x0 - 4 and x0 stay 16-byte aligned.  Tiles that reach
+// within two cells of the left or right boundary, or into a sponge layer,
+// take the general kernel, whose cost is one warp per 28-column strip holding
+// a cell; the origin is the first of the 28 aligned shifts that minimises
+// those strips (origin 0 when no shift does better).  Periodic grids and
+// grids narrower than 2 kTileX + 4 keep origin 0.
+inline int tile_origin(int nx, bool periodic, int sp_left, int sp_right)
+{
+    if (periodic || nx < 2 * kTileX + 4) return 0;
+    const int need_l = sp_left > 2 ? sp_left : 2, need_r = sp_right > 2 ? sp_right : 2;
+    int best = 0, best_cost = -1;
+    for (int org = 0; org > -kTileX; org -= 4) {
+        const int tiles = (nx - org + kTileX - 1) / kTileX;
+        int cost = 0;
+        for (int t = 0; t < tiles; t++) {
+            const int x0 = org + t * kTileX;
+            if (x0 >= need_l && x0 + kTileX <= nx - need_r) continue;   // may run deep
+            for (int k = 0; k < kTileX / 28; k++) cost += (x0 + 28 * k + 28 > 0 && x0 + 28 * k < nx) ? 1 : 0;
+        }
+        if (best_cost < 0 || cost < best_cost) {
+            best_cost = cost;
+            best = org;
+        }
+    }
+    return best;
+}
+
 // Warp tilings of the stepping kernels, picked per workload by the autotuner
 // (runtime/tuner.cu).  A work unit is always kTileX x kHalfRows cells, each
 // of its four column strips marched by warps; a tiling says into how many row

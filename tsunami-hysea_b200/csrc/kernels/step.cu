@@ -272,8 +272,9 @@ __device__ __forceinline__ void y_edge(const ScenarioDev &s, const Cell &m, cons
 
 // ---------------------------------------------------------------------------
 // Work units and their classes.  A unit is a half tile (kTileX x kHalfRows
-// cells); work-list entry w (scenario, tile) holds units 2w (upper half) and
-// 2w+1 (lower half).  Phase 1 records each unit's depth summary (UnitSum);
+// cells; tile column tx starts at grid column x_org + tx kTileX, so tile 0
+// and the last tile may hold fewer columns); work-list entry w (scenario,
+// tile) holds units 2w (upper half) and 2w+1 (lower half).  Phase 1 records each unit's depth summary (UnitSum);
 // from the unit's own cells and the border strips and corners of its eight
 // neighbours - exactly its two-cell stencil ring -
 //   deep:  every cell of unit and ring deeper than hpos, and the unit at
@@ -292,7 +293,7 @@ __device__ __forceinline__ int units_y(const ScenarioDev &s) { return (s.ny + kH
 __device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const UnitSum *__restrict__ sum, int tx, int uy)
 {
     if (!s.tmap) return false;
-    const int x0 = tx * kTileX, yb = uy * kHalfRows;
+    const int x0 = s.x_org + tx * kTileX, yb = uy * kHalfRows;
     if (x0 < max(2, s.sp_left) || x0 + kTileX > s.nx - max(2, s.sp_right)) return false;
     if (yb < max(2, s.sp_up) || yb + kHalfRows > s.ny - max(2, s.sp_low)) return false;
     const int W = s.tiles_x;
@@ -495,6 +496,7 @@ constexpr int SPLANE = (kStageRows * kStageW + 31) / 32 * 32;   // floats per st
 constexpr int DPLANE = kHalfRows * kTileX;          // floats per staged diagnostics plane
 constexpr uint32_t kStateBytes = kStageRows * kStageW * 4;
 constexpr uint32_t kDiagBytes = kHalfRows * kTileX * 4;
+// x0 = x_org + tx kTileX with x_org a multiple of 4 (tile_origin)
 static_assert(kTileX % 4 == 0, "TMA x coordinates x0 - 4 and x0 must be 16-byte aligned");
 static_assert(kTileY == 2 * kHalfRows, "two half tiles per tile");
 static_assert((SPLANE * 4) % 128 == 0 && (DPLANE * 4) % 128 == 0, "staged planes 128-byte aligned");
@@ -798,7 +800,7 @@ __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ sc
     const int ty = item.y / d.s->tiles_x, tx = item.y - ty * d.s->tiles_x;
     const int uy = 2 * ty + (u & 1);
     d.uidx = uy * d.s->tiles_x + tx;
-    d.x0 = tx * kTileX;
+    d.x0 = d.s->x_org + tx * kTileX;
     d.yb = uy * kHalfRows;
     const ScenarioDev &s = *d.s;
     ScenarioCtl *ctl = s.ctl;
@@ -1228,14 +1230,14 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
         if (uy0 >= ny) continue;   // a unit below the grid (phase 0 only; never listed)
         const int unit_end = min(uy0 + kHalfRows, ny);
         // this warp: column strip `strip`, rows y0 .. y_end-1 of the unit
-        const int x0 = tx * kTileX + strip * OUTW, y0 = uy0 + group * GROWS;
+        const int x0 = s.x_org + tx * kTileX + strip * OUTW, y0 = uy0 + group * GROWS;
         const int p = ctl->parity;
         const float dt = (float)ctl->dt;
         const float t_sec = (float)(ctl->t * ctl->T);
         const int gx = x0 - 2 + lane;
         const int col = map_col(gx, nx, s.periodic);
-        const bool has_edge = (lane >= 2) && (lane <= 30) && (gx <= nx);
-        const bool has_cell = (lane >= 2) && (lane <= 29) && (gx < nx);
+        const bool has_edge = (lane >= 2) && (lane <= 30) && (gx >= 0) && (gx <= nx);
+        const bool has_cell = (lane >= 2) && (lane <= 29) && (gx >= 0) && (gx < nx);
         const int y_end = min(y0 + GROWS, unit_end);
         const float *eta_in = (PHASE == 2) ? s.eta[p ^ 1] : s.eta[p];
         const float *qx_in = s.qx[p], *qy_in = s.qy[p];
@@ -1248,7 +1250,7 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
         hacc.init();
         bool bad = false;
 
-        if (x0 < nx && y0 < y_end) {
+        if (x0 < nx && x0 + OUTW > 0 && y0 < y_end) {
             constexpr bool DIAG = (PHASE == 1);
             Cell c0 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 2, ny) * pitch + col);
             Cell c1 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 1, ny) * pitch + col);
@@ -1455,8 +1457,8 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
         // ---- unit reductions: phase 1 depth summary -> usum; phase 0/2 dt -> scenario min ----
         if (PHASE == 1) {
             // the unit's first two and last two columns inside the grid
-            const int ux0 = tx * kTileX, ux1 = min(ux0 + kTileX, nx);
-            const bool cell = has_cell && x0 < nx;
+            const int tx0 = s.x_org + tx * kTileX, ux0 = max(tx0, 0), ux1 = min(tx0 + kTileX, nx);
+            const bool cell = has_cell && x0 < nx && x0 + OUTW > 0;
             warp_unit_summary(hacc, cell, cell && gx < ux0 + 2, cell && gx >= ux1 - 2, slots + 9 * warp);
         } else {
             for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));

@@ -138,7 +138,7 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
     size_t b = 10 * pitch * ny * sizeof(float);          // fields
     b += (size_t)(5 * ny + 1) * sizeof(float);           // row tables
     b += 3 * (size_t)nx * ny * sizeof(float);            // output staging
-    b += 2 * (size_t)((nx + kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(UnitSum) + 1);
+    b += 2 * (size_t)((nx + 2 * kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(UnitSum) + 1);
     b += kNumMaps * sizeof(TmaMap) + (size_t)(ny + 1) * sizeof(float4);
     if (has_faults) b += (size_t)nx * ny * sizeof(double);
     return b + 4096;
@@ -254,7 +254,10 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.nx = nx;
     desc.ny = ny;
     desc.pitch = pitch;
-    desc.tiles_x = (nx + kTileX - 1) / kTileX;
+    desc.periodic = (std::fabs(p->border_left - 2.0) < 2.220446049250313e-16) &&
+                    (std::fabs(p->border_right - 2.0) < 2.220446049250313e-16);
+    desc.x_org = tile_origin(nx, desc.periodic != 0, p->sponge_left, p->sponge_right);
+    desc.tiles_x = (nx - desc.x_org + kTileX - 1) / kTileX;
     desc.tiles_y = (ny + kTileY - 1) / kTileY;
     desc.ntiles = desc.tiles_x * desc.tiles_y;
     THY_CK(cudaMallocAsync(&usum, 4 * (size_t)desc.ntiles * sizeof(UnitSum), st));
@@ -262,8 +265,6 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.usum[0] = usum;
     desc.usum[1] = usum + 2 * desc.ntiles;
     desc.dry_age = dry_age;
-    desc.periodic = (std::fabs(p->border_left - 2.0) < 2.220446049250313e-16) &&
-                    (std::fabs(p->border_right - 2.0) < 2.220446049250313e-16);
     desc.b_up = (float)p->border_up;
     desc.b_low = (float)p->border_low;
     desc.b_left = (float)p->border_left;
