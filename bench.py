@@ -245,7 +245,8 @@ def run_ours(a, dist: Dist):
     # per-kernel device time for the roofline (individually launched steps);
     # each kernel's algorithmic bytes count the cells it steps: deep units are
     # interior units of UNIT_CELLS cells, dry land units are skipped, the
-    # general kernels step the rest
+    # general kernels step the rest (a dry unit counts as UNIT_CELLS cells;
+    # boundary units can be narrower, so the general count is a lower bound)
     t0_units, t0_deep, t0_dry = sess.tiles()
     prof_steps = 32
     ms6 = sess.profile_launches(prof_steps)

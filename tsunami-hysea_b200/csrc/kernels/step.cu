@@ -217,18 +217,19 @@ __device__ void controller(const ScenarioDev &s)
 
 // Edge between rows gy-1 (a) and gy (b) of this lane's column, stencil rows
 // gy-2 .. gy+1 = (m, a, b, p).  "u" is qy (normal), "v" qx (tangential).
+// ka, kb: row metrics {cos, ilcos, area, dlon} of rows clamp(gy-1) and
+// clamp(gy); dlon: the edge row's length (rowpack[gy].w).
 __device__ __forceinline__ void gather_y(Edge &e, const ScenarioDev &s, const Cell &m, const Cell &a, const Cell &b,
-                                         const Cell &p, int gy)
+                                         const Cell &p, int gy, const float4 &ka, const float4 &kb, float dlon)
 {
     e.h0m = m.h; e.h0 = a.h; e.h1 = b.h; e.h1p = p.h;
     e.e0m = m.e; e.e0 = a.e; e.e1 = b.e; e.e1p = p.e;
     e.D0 = a.D; e.D1 = b.D;
     e.u0m = m.qy; e.u0 = a.qy; e.u1 = b.qy; e.u1p = p.qy;
     e.v0m = m.qx; e.v0 = a.qx; e.v1 = b.qx; e.v1p = p.qx;
-    const int ra = clamp_row(gy - 1, s.ny), rb = clamp_row(gy, s.ny);
-    e.area0 = __ldg(s.row.area + ra); e.cos0 = __ldg(s.row.cosphi + ra);
-    e.area1 = __ldg(s.row.area + rb); e.cos1 = __ldg(s.row.cosphi + rb);
-    e.len = __ldg(s.row.dlon + gy);
+    e.area0 = ka.z; e.cos0 = ka.x;
+    e.area1 = kb.z; e.cos1 = kb.x;
+    e.len = dlon;
     e.normal = 1.f;
     e.front = false;
     if (gy == 0) {
@@ -248,10 +249,11 @@ struct Contrib {
 
 template <int PHASE>
 __device__ __forceinline__ void y_edge(const ScenarioDev &s, const Cell &m, const Cell &a, const Cell &b, const Cell &p,
-                                       int gy, float dt, Contrib &lo, Contrib &hi)
+                                       int gy, float dt, Contrib &lo, Contrib &hi, const float4 &ka, const float4 &kb,
+                                       float dlon)
 {
     Edge e;
-    gather_y(e, s, m, a, b, p, gy);
+    gather_y(e, s, m, a, b, p, gy, ka, kb, dlon);
     const bool ghost_lo = (gy == 0);
     if (PHASE == 1) {
         const float F = mass_flux<true>(e, s, dt);
@@ -1274,17 +1276,23 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
             RawCell n1 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 3, ny) * pitch + col,
                                         has_cell && y0 + 3 < y_end);
             // y edge at the top of the first row (stencil rows y0-2 .. y0+1)
+            // row metrics {cos, ilcos, area, dlon} (rowpack), loaded a row
+            // ahead: kc of row yo, kn of row yo+1 (entry ny: dlon only)
+            const float4 *__restrict__ rp = s.rowpack;
+            float4 kc = __ldg(rp + y0);
+            float4 kn = __ldg(rp + y0 + 1);
             Contrib top, dummy;
-            y_edge<PHASE>(s, c0, c1, c2, c3, y0, dt, dummy, top);
+            y_edge<PHASE>(s, c0, c1, c2, c3, y0, dt, dummy, top, __ldg(rp + clamp_row(y0 - 1, ny)), kc, kc.w);
 
             for (int yo = y0; yo < y_end; yo++) {
+                const float4 knn = __ldg(rp + min(yo + 2, ny));
                 // rows yo+3 (loaded an iteration ago) and yo+4 (now) are in flight
                 const RawCell n2 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(yo + 4, ny) * pitch + col,
                                                   has_cell && yo + 4 < y_end);
                 const size_t idx = (size_t)yo * pitch + col;
                 // ---- y edge below this row (between yo and yo+1) ----
                 Contrib below, next_top;
-                y_edge<PHASE>(s, c1, c2, c3, c4, yo + 1, dt, below, next_top);
+                y_edge<PHASE>(s, c1, c2, c3, c4, yo + 1, dt, below, next_top, kc, (yo + 1 < ny) ? kn : kc, kn.w);
 
                 // ---- x edge left of this lane's cell (row yo) ----
                 Edge e;
@@ -1312,10 +1320,10 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
                     e.v0m = e.v0 = e.v1p = e.v1 = 0.f;
                 }
                 e.u0m = e.u1p = 0.f;
-                const float area = __ldg(s.row.area + yo);
+                const float area = kc.z;
                 e.area0 = e.area1 = area;
-                e.cos0 = e.cos1 = __ldg(s.row.cosphi + yo);
-                e.len = __ldg(s.row.ilcos + yo);
+                e.cos0 = e.cos1 = kc.x;
+                e.len = kc.y;
                 e.normal = 1.f;
                 e.front = false;
                 if (x_ghost_lo) {
@@ -1443,6 +1451,8 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
                     }
                 }
                 top = next_top;
+                kc = kn;
+                kn = knn;
                 c0 = c1;
                 c1 = c2;
                 c2 = c3;
