@@ -3,8 +3,8 @@
 // TEST INFRASTRUCTURE ONLY (an oracle).  Nothing in the product links,
 // loads or calls this file.  It is built by oracle/Makefile into
 // oracle/_ref/librefemu.so from the reference sources where they lie
-// (REF_SRC, default /root/reference/src); no reference source is copied
-// into this repository.
+// (REF_SRC, the reference's src directory, set by oracle/Makefile); no
+// reference source is copied into this repository.
 //
 // What is the reference's and what is this harness's:
 //   - every __global__/__device__ function (edge fluxes, cell updates,
