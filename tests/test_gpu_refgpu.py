@@ -13,11 +13,13 @@ has the reference's command line and output files.
   the time step (src/GPU/Reduccion_kernel.cu:130-160) skips its second pass
   whenever the first pass's block count is not a power of two, and its dt is
   then the minimum over a subset of the cells;
-* head to head on the single large workload (4096 x 4096 cells, four Okada
-  subfaults, 3600 s simulated, snapshots every 1800 s): both programs print
-  their loop wall time ("Runtime: ... sec", the reference's *tiempo), which
-  includes Okada and the snapshot writes in both; cell-updates/s = cells x
-  iterations / runtime.  This library must step the same problem faster.
+* head to head on the plain small workload (512 x 512 cells, one Okada
+  fault, 600 s simulated, snapshots every 300 s) and the single large one
+  (4096 x 4096 cells, four Okada subfaults, 3600 s, snapshots every 1800 s):
+  both programs print their loop wall time ("Runtime: ... sec", the
+  reference's *tiempo), which includes Okada and the snapshot writes in both;
+  cell-updates/s = cells x iterations / runtime.  This library must step the
+  same problem faster.
 """
 import json
 import os
@@ -92,14 +94,24 @@ def test_parity_with_reference_cuda_build(refgpu, tmp_path):
     _compare(got, ref)
 
 
-def test_head_to_head_single_large(refgpu, tmp_path):
-    p = synth.single_large(n=4096, sim_time=3600.0, save_time=1800.0)
-    p.name = "refgpu_large"
+HEAD_TO_HEAD = {
+    "plain_small_512": ("plain_small 512x512, 1 Okada fault, 600 s, snapshots every 300 s",
+                        lambda: synth.plain_small(nx=512, ny=512, sim_time=600.0, save_time=300.0, npoints=16)),
+    "single_large_4096": ("single_large 4096x4096, 4 Okada subfaults, 3600 s, snapshots every 1800 s",
+                          lambda: synth.single_large(n=4096, sim_time=3600.0, save_time=1800.0)),
+}
+
+
+@pytest.mark.parametrize("workload", sorted(HEAD_TO_HEAD))
+def test_head_to_head(refgpu, tmp_path, workload):
+    name, make = HEAD_TO_HEAD[workload]
+    p = make()
+    p.name = "refgpu_" + workload
     ref, ref_s, ref_it = _run(refgpu, p, str(tmp_path / "ref"))
     got, got_s, got_it = _run(CLI, p, str(tmp_path / "got"))
     cells = p.nx * p.ny
     eta_err, maxh_err = _compare(got, ref, gauges=False, same_times=False)
-    rec = {"workload": "single_large 4096x4096, 4 Okada subfaults, 3600 s, snapshots every 1800 s",
+    rec = {"workload": name,
            "reference_cuda": {"runtime_s": ref_s, "iterations": ref_it, "cell_updates_per_s": cells * ref_it / ref_s},
            "thysea": {"runtime_s": got_s, "iterations": got_it, "cell_updates_per_s": cells * got_it / got_s},
            "max_abs_eta_m": eta_err, "max_height_rel_l2": maxh_err}
