@@ -99,52 +99,67 @@ class Dist:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+    """SM clock and clock-event (throttle) reasons of this rank's GPU, read
+    through NVML by a background thread every `period` seconds while the
+    timed work runs (the library's calls release the GIL).  The NVML device
+    is the one CUDA_VISIBLE_DEVICES maps this rank's device to."""
 
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
-         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
-         "clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, device: int):
+    def __init__(self, device: int, period: float = 0.002):
         self.device = device
-        self.proc = None
-        self.path = None
+        self.period = period
+        self.thread = None
+        self.samples = []
+        self.error = None
+
+    def _handle(self, nv):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES", "").strip()
+        ids = [x.strip() for x in vis.split(",") if x.strip()] if vis else []
+        if self.device < len(ids):
+            x = ids[self.device]
+            if x.isdigit():
+                return nv.nvmlDeviceGetHandleByIndex(int(x))
+            return nv.nvmlDeviceGetHandleByUUID(x)
+        return nv.nvmlDeviceGetHandleByIndex(self.device)
 
     def start(self):
-        fd, self.path = tempfile.mkstemp(prefix="clocks_", suffix=".csv")
-        os.close(fd)
+        import threading
+
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
-        except OSError:
-            self.proc = None
+            import pynvml as nv
+
+            nv.nvmlInit()
+            h = self._handle(nv)
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+        except Exception as e:  # noqa: BLE001
+            self.error = f"NVML unavailable: {e}"
+            return
+        self.stop_flag = threading.Event()
+
+        def loop():
+            while not self.stop_flag.is_set():
+                try:
+                    self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                         int(nv.nvmlDeviceGetCurrentClocksEventReasons(h))))
+                except Exception as e:  # noqa: BLE001
+                    self.error = str(e)
+                    return
+                self.stop_flag.wait(self.period)
+
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
 
     def stop(self) -> dict:
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except subprocess.TimeoutExpired:
-            self.proc.kill()
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in open(self.path):
-            f = [x.strip() for x in line.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for n, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(n)
-        os.unlink(self.path)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+        if self.thread is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [self.error or "not sampled"], "samples": 0}
+        self.stop_flag.set()
+        self.thread.join(timeout=5)
+        sm = [s for s, _ in self.samples]
+        reasons = sorted({n for _, r in self.samples for n, bit in self.REASONS if r & bit})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz, "reasons": reasons,
+                "samples": len(sm), "period_ms": self.period * 1e3, "source": "NVML"}
 
 
 def measured_peak():
@@ -282,6 +297,8 @@ def run_ours(a, dist: Dist):
         outs = thysea.PinnedOutputs(prep)
         thysea.run(prep, snapshots=False, series=False, out=outs.fields)  # warm-up run
         times, steps_run, parts = [], 0, []
+        clk_e2e = ClockSampler(dist.local)
+        clk_e2e.start()
         for _ in range(a.e2e_runs):
             dist.barrier()
             t0 = time.perf_counter()
@@ -290,6 +307,7 @@ def run_ours(a, dist: Dist):
             steps_run = out["iterations"]
             parts.append((out["setup_seconds"], out["loop_seconds"], out["device_ms"] / 1e3, out["output_seconds"],
                           out["total_seconds"], out["release_seconds"]))
+        clocks_e2e = clk_e2e.stop()
         t = dist.max(statistics.mean(times))
         e2e = {"value": round(dist.sum(float(cells * steps_run)) / t, 1), "unit": METRIC,
                "h2d_bytes_per_step": int(32 * cells + 4 * (5 * p.ny + 1) + 80 * len(p.faults)),
@@ -301,7 +319,7 @@ def run_ours(a, dist: Dist):
                "loop_device_s": round(statistics.mean(x[2] for x in parts), 4),
                "output_s": round(statistics.mean(x[3] for x in parts), 4),
                "library_call_s": round(statistics.mean(x[4] for x in parts), 4),
-               "release_s": round(statistics.mean(x[5] for x in parts), 4)}
+               "release_s": round(statistics.mean(x[5] for x in parts), 4), "clocks": clocks_e2e}
     cpu = None
     if dist.rank == 0 and dist.world == 1 and not a.skip_cpu:
         try:
@@ -608,7 +626,7 @@ def run_tilings(a, dist):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=960, help="timed time steps (multiple of 16)")
+    ap.add_argument("--steps", type=int, default=960, help="timed time steps")
     ap.add_argument("--warmup", type=int, default=32)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--n", type=int, default=4096, help="grid side")

@@ -141,6 +141,11 @@ typedef struct thy_stats {
     thy_tiling tiling;        /* the warp tiling of the loop's last chunk */
     long long tune_samples;   /* chunks of the loop timed for the autotuner */
     double release_seconds;   /* release of the device buffers, graphs and streams after the outputs */
+    long long chunks;         /* graph launches of the time loop */
+    long long graph_captures; /* step graphs captured (per tiling and chunk length) */
+    double capture_seconds;   /* host time spent capturing and instantiating them */
+    double event_seconds;     /* host time spent on the loop's events (faults, snapshots, gauges) */
+    double initial_seconds;   /* initial dt and the t = 0 faults, before the first chunk */
 } thy_stats;
 
 /* Library / device. */
@@ -198,8 +203,10 @@ int thy_apply_okada(int nx, int ny, double lon0, double dlon, double lat0, doubl
  * (8 MiB) held by every GPU that loads the library until the process exits;
  * larger grids return THY_ERR_TOO_LARGE.  The first call on a device looks
  * up that array's device address, so it should come before any stream
- * capture.  The call only enqueues the work on `stream`.  All calls share
- * the scratch: calls whose work overlaps on the GPU race. */
+ * capture; after a device reset (cudaDeviceReset) the addresses are looked
+ * up again by the next call, which then counts as a first call.  The call
+ * only enqueues the work on `stream`.  All calls share the scratch: calls
+ * whose work overlaps on the GPU race. */
 #define THY_OKADA_NOALLOC_MAX_CELLS (1 << 20)
 int thy_apply_okada_noalloc(int nx, int ny, double lon0, double dlon, double lat0, double dlat, const double *fault,
                             double H, int crop_flag, double crop_value, void *d_state1, double *d_eta_initial,
@@ -233,7 +240,7 @@ int thy_session_tuned(const thy_session *s, thy_tiling *best);
 void thy_session_close(thy_session *s);
 /* Test hook for failure detection: with `what` = 1 the deep-water kernels
    issue none of this session's staging copies, so their bounded waits
-   (about half a second) run out, the step stops and thy_session_steps
+   (four seconds of global time) run out, the step stops and thy_session_steps
    returns THY_ERR_TIMEOUT with the device context still usable; 0 turns it
    off.  Nothing faults, traps or hangs. */
 int thy_session_inject(thy_session *s, int what);

@@ -1,5 +1,5 @@
 """Failure detection on the GPU without a fault: every wait of the deep-water
-kernels is bounded (about half a second), so a staging copy that does not
+kernels is bounded (four seconds of global time), so a staging copy that does not
 land stops the step with THY_ERR_TIMEOUT instead of hanging.  The test hook
 thy_session_inject makes the kernels issue none of a session's copies (a
 flag that nothing sets); afterwards the context still runs other work, with

@@ -83,7 +83,7 @@ def test_netcdf_files_written_from_many_threads():
     (the snapshot writers of several scenarios do this)"""
     from scipy.io import netcdf_file
 
-    L = _ffi.lib()
+    L = _ffi.nclite()
     d = tempfile.mkdtemp()
     errors = []
 

@@ -36,6 +36,18 @@ def test_header_symbols_are_exported():
     assert set(_ffi.SIGNATURES) <= names
 
 
+def test_only_the_c_abi_is_exported():
+    """libthysea.so exports the C ABI and shallowWater and nothing else: in
+    particular not the nc_* functions of its built-in NetCDF code, so that a
+    program that also links a real libnetcdf keeps that library's calls"""
+    so = os.path.join(ROOT, "tsunami-hysea_b200", "lib", "libthysea.so")
+    out = subprocess.run(["nm", "-D", "--defined-only", so], capture_output=True, text=True, check=True).stdout
+    syms = [ln.split()[-1] for ln in out.splitlines() if ln.split() and ln.split()[-2] in ("T", "D", "B", "W", "V")]
+    assert "shallowWater" in syms and "thy_run" in syms
+    assert [s for s in syms if not (s.startswith("thy_") or s == "shallowWater")] == []
+    assert not [s for s in syms if s.startswith("nc_")]
+
+
 def test_no_device_fails_loudly():
     L = _ffi.lib()
     if L.thy_device_count() > 0:
@@ -131,7 +143,7 @@ def test_nclite_roundtrip_with_scipy():
     """files written through the library's NetCDF API read back with scipy and vice versa"""
     from scipy.io import netcdf_file
 
-    L = _ffi.lib()
+    L = _ffi.nclite()
     d = tempfile.mkdtemp()
     path = os.path.join(d, "t.nc").encode()
     nc, dx, dt, vx, vt = (ctypes.c_int() for _ in range(5))

@@ -39,6 +39,8 @@ CUDA_SOURCES = [
     "host/problem.cpp",
 ]
 C_SOURCES = ["nclite/nclite.c"]
+# the library's exported symbols: the C ABI and shallowWater only
+EXPORTS = os.path.join(CSRC, "exports.map")
 # FP32 stepping kernels: approximate division / sqrt / exp (<= 2 ulp); the FP64
 # Okada and set-up kernels keep IEEE arithmetic
 FAST_MATH = {"kernels/step.cu"}
@@ -98,11 +100,21 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
     with cf.ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), sources))
     so = os.path.join(LIB, "libthysea.so")
-    if not os.path.exists(so) or any(os.path.getmtime(o) > os.path.getmtime(so) for o in objs):
-        cmd = [NVCC, *ARCH, "-shared", "-o", so, *objs]
+    if not os.path.exists(so) or any(os.path.getmtime(o) > os.path.getmtime(so) for o in objs + [EXPORTS]):
+        cmd = [NVCC, *ARCH, "-shared", "-o", so, *objs, "-Xlinker", "--version-script=" + EXPORTS]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    # nclite on its own, with the NetCDF C API exported: for programs that
+    # call nc_* themselves (the reference's own writers relinked against this
+    # library, the tests of the NetCDF code); libthysea.so keeps its copy private
+    nclite_so = os.path.join(LIB, "libnclite.so")
+    nclite_src = os.path.join(CSRC, "nclite", "nclite.c")
+    if not os.path.exists(nclite_so) or os.path.getmtime(nclite_src) > os.path.getmtime(nclite_so):
+        cmd = ["gcc", "-O2", "-fPIC", "-shared", "-std=c11", "-Wall", *INCLUDES, nclite_src, "-o", nclite_so]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError(f"compile failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
     main_src = os.path.join(CSRC, "host", "main.cpp")
     exe = os.path.join(BIN, "TsunamiHySEA")
     if os.path.exists(main_src) and (not os.path.exists(exe) or os.path.getmtime(so) > os.path.getmtime(exe)

@@ -445,7 +445,6 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-// at most 2^20 polls (each try_wait may suspend the thread for a while)
 __device__ __forceinline__ unsigned long long global_ns()
 {
     unsigned long long t;
@@ -453,15 +452,20 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
-// waits for the phase with this parity to complete; false after about half a
-// second (the copies it waits for did not land), so that no wait is endless
+// Waits for the phase with this parity to complete; false when it has not
+// after kWaitNs of global time or 2^28 polls, whichever comes first (each
+// try_wait may suspend the thread for a while), so that no wait is endless.
+// A staging copy lands within microseconds; the limit is seconds so that a
+// context that is time-sliced or pre-empted on a shared GPU does not take a
+// healthy copy for a lost one.
+constexpr unsigned long long kWaitNs = 4000000000ull;
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
-    for (int i = 0; i < (1 << 24); i++) {
+    for (int i = 0; i < (1 << 28); i++) {
         if (mbar_try_wait(bar, parity)) return true;
-        if (global_ns() - t0 > 500000000ull) return false;
+        if (global_ns() - t0 > kWaitNs) return false;
     }
     return false;
 }

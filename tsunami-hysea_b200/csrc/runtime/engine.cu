@@ -832,7 +832,7 @@ int Batch::update(const std::vector<char> *selected)
 
 void Batch::drop_graphs()
 {
-    for (auto &g : graphs) cudaGraphExecDestroy(g.second);
+    for (auto &g : graphs) cudaGraphExecDestroy(g.exec);
     graphs.clear();
     gexec = nullptr;
 }
@@ -842,8 +842,8 @@ int Batch::use_tiling(const Tiling &t)
     if (gexec && t == tiling) return THY_OK;
     tiling = t;
     for (auto &g : graphs)
-        if (g.first == t) {
-            gexec = g.second;
+        if (g.tiling == t && g.len == chunk) {
+            gexec = g.exec;
             return THY_OK;
         }
     return capture();
@@ -852,23 +852,27 @@ int Batch::use_tiling(const Tiling &t)
 // Grids depend on the work-list capacity and the tiling only, so a graph
 // survives changes of the member set (the kernels read the table and the
 // lists from device memory).
-int Batch::capture()
+int Batch::capture(int len)
 {
+    if (len <= 0 || len > chunk) len = chunk;
+    const auto t_cap = std::chrono::steady_clock::now();
     for (size_t i = 0; i < graphs.size(); i++)
-        if (graphs[i].first == tiling) {
-            cudaGraphExecDestroy(graphs[i].second);
+        if (graphs[i].tiling == tiling && graphs[i].len == len) {
+            if (graphs[i].exec == gexec) gexec = nullptr;
+            cudaGraphExecDestroy(graphs[i].exec);
             graphs.erase(graphs.begin() + i);
             break;
         }
-    gexec = nullptr;
+    if (len == chunk) gexec = nullptr;
     // Each phase's general and deep-water kernels step disjoint tiles and
     // share only atomically updated scenario fields, so they are two
     // branches of the graph: the deep tiles fill the SMs the general
     // kernel's last wave leaves idle.
     const StepLaunch L = params();
     cudaGraph_t g;
+    cudaGraphExec_t exec = nullptr;
     THY_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    for (int k = 0; k < chunk; k++) {
+    for (int k = 0; k < len; k++) {
         for (int ph = 0; ph < 2; ph++) {
             THY_CK(cudaEventRecord(ev_fork, st));
             THY_CK(cudaStreamWaitEvent(st_side, ev_fork, 0));
@@ -881,11 +885,35 @@ int Batch::capture()
         launch_step_kernel(5, L, st);                     // controller
     }
     THY_CK(cudaStreamEndCapture(st, &g));
-    cudaError_t e = cudaGraphInstantiate(&gexec, g, 0);
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
     cudaGraphDestroy(g);
     THY_CK(e);
-    graphs.emplace_back(tiling, gexec);
+    graphs.push_back(Graph{tiling, len, exec});
+    if (len == chunk) gexec = exec;
+    captures++;
+    capture_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - t_cap).count();
     return THY_OK;
+}
+
+long long Batch::steps_to_event(const DevScenario &s)
+{
+    const ScenarioCtl &c = s.hctl;
+    double horizon = c.t_end;
+    if (c.save_nc >= 0.0) horizon = std::min(horizon, c.next_nc);
+    if (c.save_ts >= 0.0) horizon = std::min(horizon, c.next_ts);
+    const int nf = (int)(s.faults.size() / 10);
+    if (c.fault_next < nf) horizon = std::min(horizon, s.faults[10 * c.fault_next] / s.Ts);
+    long long n = (c.dt > 0.0) ? (long long)std::ceil((horizon - c.t) / c.dt) : 1;
+    if (c.max_steps >= 0) n = std::min(n, c.max_steps - c.step);
+    return std::max(1ll, n);
+}
+
+int Batch::chunk_for(long long steps) const
+{
+    if (steps >= chunk) return chunk;
+    int len = 1;
+    while (2 * len <= steps) len *= 2;
+    return len;
 }
 
 int Batch::rebuild()
@@ -942,12 +970,23 @@ TuneKey Batch::tune_key(bool *known, bool all_members) const
     return TuneKey{device, tune_bucket(deep), tune_bucket(general)};
 }
 
-int Batch::run_chunk(bool timed)
+int Batch::run_chunk(bool timed, int len)
 {
     int rc;
     bool sampling = false, known = false;
+    if (len <= 0 || len > chunk) len = chunk;
     const TuneKey key = tune_key(&known);
     if ((rc = use_tiling(tuner_pick(key, &sampling)))) return rc;
+    cudaGraphExec_t exec = gexec;
+    if (len != chunk) {
+        exec = nullptr;
+        for (auto &g : graphs)
+            if (g.tiling == tiling && g.len == len) exec = g.exec;
+        if (!exec) {
+            if ((rc = capture(len))) return rc;
+            exec = graphs.back().exec;
+        }
+    }
     // a sample needs a chunk in which every running member steps `chunk`
     // times (no member reaches its end or an event before the chunk's last
     // step, none fails) and whose work mix was known beforehand
@@ -963,7 +1002,7 @@ int Batch::run_chunk(bool timed)
             running++;
         }
     if (timed) THY_CK(cudaEventRecord(ev0, st));
-    THY_CK(cudaGraphLaunch(gexec, st));
+    THY_CK(cudaGraphLaunch(exec, st));
     if (timed) THY_CK(cudaEventRecord(ev1, st));
     THY_CK(cudaMemcpyAsync(h_ctl, d_ctl, capacity * sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, st));
     THY_CK(cudaStreamSynchronize(st));
@@ -972,8 +1011,9 @@ int Batch::run_chunk(bool timed)
         THY_CK(cudaEventElapsedTime(&ms, ev0, ev1));
         device_ms += ms;
     }
-    launches += (long long)kLaunchesPerStep * chunk;
-    bool full = running > 0;
+    launches += (long long)kLaunchesPerStep * len;
+    chunks_run++;
+    bool full = running > 0 && len == chunk;
     double stepped = 0;   // deep + general units stepped in the chunk
     for (int i = 0; i < capacity; i++) {
         DevScenario *m = members[i];
@@ -1162,6 +1202,8 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
     THY_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
     auto t0 = std::chrono::steady_clock::now();
     auto t_release = t0;
+    double event_s = 0;
+    if (stats) std::memset(stats, 0, sizeof(*stats));
     {
         DevScenario s;
         Batch b;
@@ -1173,20 +1215,26 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
         t0 = std::chrono::steady_clock::now();
         if (stats) stats->setup_seconds = std::chrono::duration<double>(t0 - t_start).count();
         if ((rc = initial_dt(b))) goto out;
+        if (stats) stats->initial_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
         for (;;) {
             if (!(s.hctl.t < s.t_end)) break;
             if (s.max_steps >= 0 && s.hctl.step >= s.max_steps) break;
             if (s.hctl.status == kFailed) { rc = failure_code(s.hctl); goto out; }
             {
+                const auto te = std::chrono::steady_clock::now();
                 bool changed = false;
                 if ((rc = handle_events_ex(s, o, st, &changed))) goto out;
                 if (changed && (rc = b.reset_lists())) goto out;
+                event_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - te).count();
             }
             s.hctl.status = kRunning;
             s.hctl.events = 0;
             if ((rc = s.upload_ctl(st))) goto out;
+            // chunks no longer than the steps left before the next event (as
+            // far as the current dt tells), so that few launches find the
+            // scenario paused
             do {
-                if ((rc = b.run_chunk(true))) goto out;
+                if ((rc = b.run_chunk(true, b.chunk_for(Batch::steps_to_event(s))))) goto out;
             } while (s.hctl.status == kRunning);
             if (s.hctl.status == kFailed) { rc = failure_code(s.hctl); goto out; }
         }
@@ -1206,6 +1254,10 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
                 stats->dry_tiles = (long long)s.hctl.units_dry;
                 stats->tiling = thy_tiling{b.tiling.deep1, b.tiling.deep2, b.tiling.general};
                 stats->tune_samples = b.tune_samples;
+                stats->chunks = b.chunks_run;
+                stats->graph_captures = b.captures;
+                stats->capture_seconds = b.capture_s;
+                stats->event_seconds = event_s;
             }
         }
         {
@@ -1271,9 +1323,12 @@ extern "C" int thy_session_steps(thy_session *S, long long steps, double *device
         s.hctl.status = kRunning;
         s.hctl.events = 0;
         if ((rc = s.upload_ctl(S->st))) return rc;
+        // exactly `steps` steps' launches: full chunks, then power-of-two
+        // chunks for the rest (a scenario that reaches its end or a fault
+        // time earlier stops there)
         do {
-            if ((rc = S->b.run_chunk(true))) return rc;
-        } while (s.hctl.status == kRunning);
+            if ((rc = S->b.run_chunk(true, S->b.chunk_for(start + steps - s.hctl.step)))) return rc;
+        } while (s.hctl.status == kRunning && s.hctl.step < start + steps);
     }
     if (device_ms) *device_ms = S->b.device_ms - ms0;
     if (steps_done) *steps_done = s.hctl.step - start;

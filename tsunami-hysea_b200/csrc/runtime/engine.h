@@ -113,7 +113,15 @@ struct Batch {
     int chunk = 16;
     int device = 0;
     Tiling tiling;                     // of gexec
-    std::vector<std::pair<Tiling, cudaGraphExec_t>> graphs;   // captured per tiling, current capacity
+    // step graphs captured for the current capacity, per tiling and length:
+    // the full chunk, and the shorter power-of-two chunks that make a step
+    // count exact (a session's last steps, the steps before an event)
+    struct Graph {
+        Tiling tiling;
+        int len;
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
     long long tune_samples = 0;        // chunks timed for the autotuner
     cudaStream_t st = nullptr;
     cudaStream_t st_side = nullptr;    // second branch of the captured graph (deep-water kernels)
@@ -122,6 +130,9 @@ struct Batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     double device_ms = 0;
     long long launches = 0;
+    long long chunks_run = 0;          // graph launches
+    long long captures = 0;            // graphs captured
+    double capture_s = 0;              // host time spent capturing and instantiating them
 
     ~Batch();
     int init(int capacity, int max_work, cudaStream_t stream);
@@ -130,14 +141,24 @@ struct Batch {
     // upload the member table and the work list (of the members with
     // selected[slot] != 0, all of them without a selection) and classify
     int update(const std::vector<char> *selected = nullptr);
-    int capture();                    // (re)capture the step graph of `tiling` for the current capacity
+    // (re)capture the `len`-step graph of `tiling` for the current capacity
+    // (len 0: the full chunk, which becomes gexec)
+    int capture(int len = 0);
     int use_tiling(const Tiling &t);  // switch graphs (capturing the tiling's graph if it has none)
     void drop_graphs();
     int rebuild();                    // update(), and capture() when there is no graph yet
     int initial_dt_of(DevScenario *s);   // initial dt of one member (phase 0 over its units only)
-    // one graph launch + control download (synchronous); the tiling is the
-    // autotuner's pick, and a full timed chunk is one of its samples
-    int run_chunk(bool timed);
+    // one graph launch of `len` steps (0 or more than `chunk`: the full
+    // chunk; otherwise a power of two below it) + control download
+    // (synchronous); the tiling is the autotuner's pick, and a full timed
+    // chunk is one of its samples
+    int run_chunk(bool timed, int len = 0);
+    // steps a member can take before its next event or its end, estimated
+    // from its current dt (at least 1)
+    static long long steps_to_event(const DevScenario &s);
+    // the longest graph (a power of two, at most `chunk`) that does not
+    // overshoot `steps`
+    int chunk_for(long long steps) const;
     // the autotuner's key of the next chunk: this device, the deep and
     // general units per step estimated from each stepping member's last
     // chunk (members with status running; every member when all_members);

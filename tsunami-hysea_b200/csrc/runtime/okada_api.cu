@@ -11,6 +11,8 @@
 // callers that must not allocate device memory at all.
 #include <mutex>
 
+#include <cuda.h>
+
 #include "engine.h"
 
 namespace thy {
@@ -22,9 +24,33 @@ static __device__ __align__(256) double g_okada_scratch[THY_OKADA_NOALLOC_MAX_CE
 static __device__ __align__(256) unsigned int g_okada_scratch_max;
 
 namespace {
+// Device addresses of the two arrays, looked up once per device and context:
+// a device reset (cudaDeviceReset) or a new primary context can load the
+// module at other addresses, so a cached address is only used while the
+// context it was looked up in is still the current one.
+struct ScratchAddr {
+    CUcontext ctx = nullptr;
+    double *def = nullptr;
+    unsigned int *max = nullptr;
+};
 std::mutex g_scratch_mu;
-double *g_scratch_dev[64] = {};        // device address of g_okada_scratch, per device
-unsigned int *g_max_dev[64] = {};      // device address of g_okada_scratch_max, per device
+ScratchAddr g_scratch[64];
+
+using CtxGetCurrentFn = CUresult (*)(CUcontext *);
+CtxGetCurrentFn ctx_get_current_fn()
+{
+    static CtxGetCurrentFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+        else
+            cudaGetLastError();
+    }
+    return fn;
+}
 }  // namespace
 
 __global__ void okada_kernel(int nx, int ny, double *__restrict__ def, double lon0, double dlon, double lat0,
@@ -49,12 +75,15 @@ __global__ void apply_deformation_reference_layout(long long n, double2 *__restr
 }
 
 // Enqueues the Okada stage on `st` with caller-provided scratch: def holds
-// nx*ny doubles, max_bits one word.
+// def_cells doubles (at least nx*ny, else THY_ERR_TOO_LARGE before any
+// work), max_bits one word.
 int enqueue_okada_reference_layout(int nx, int ny, double lon0, double dlon, double lat0, double dlat,
                                    const double *fault, double H, int crop_flag, double crop_value, double2 *state,
-                                   double *eta_initial, double *def, unsigned int *max_bits, cudaStream_t st)
+                                   double *eta_initial, double *def, size_t def_cells, unsigned int *max_bits,
+                                   cudaStream_t st)
 {
     const long long n = (long long)nx * ny;
+    if (n > (long long)def_cells) return THY_ERR_TOO_LARGE;
     OkadaFault f{fault[1], fault[2], fault[3], fault[4], fault[5], fault[6], fault[7], fault[8], fault[9]};
     dim3 block(32, 4), grid((nx + 31) / 32, (ny + 3) / 4);
     okada_kernel<<<grid, block, 0, st>>>(nx, ny, def, lon0, dlon, lat0, dlat, f, H);
@@ -97,7 +126,7 @@ extern "C" int thy_apply_okada(int nx, int ny, double lon0, double dlon, double 
         return THY_ERR_GPU_MEMORY;
     }
     rc = enqueue_okada_reference_layout(nx, ny, lon0, dlon, lat0, dlat, fault, H, crop_flag, crop_value,
-                                        (double2 *)d_state1, d_eta_initial, def, mx, st);
+                                        (double2 *)d_state1, d_eta_initial, def, n, mx, st);
     cudaError_t e = cudaStreamSynchronize(st);
     cudaFree(def);
     cudaFree(mx);
@@ -112,35 +141,47 @@ extern "C" int thy_apply_okada(int nx, int ny, double lon0, double dlon, double 
 // synchronisation is not acceptable).  Up to THY_OKADA_NOALLOC_MAX_CELLS
 // cells; larger grids return THY_ERR_TOO_LARGE before any work.  The first
 // call on a device looks up the scratch's device address there
-// (cudaGetSymbolAddress), so make that first call before any stream capture.
-// The work is only enqueued on `stream`.  The scratch is shared by every
-// call and keeps the last call's contents (the cropping maximum is cleared
-// at the start of each call); calls whose work overlaps on the GPU (other
-// streams, other host threads) race on it.
+// (cudaGetSymbolAddress), so make that first call before any stream capture;
+// after a device reset the next call looks it up again (and is then again a
+// first call).  The work is only enqueued on `stream`.  The scratch is shared
+// by every call and keeps the last call's contents (the cropping maximum is
+// cleared at the start of each call); calls whose work overlaps on the GPU
+// (other streams, other host threads) race on it.
 extern "C" int thy_apply_okada_noalloc(int nx, int ny, double lon0, double dlon, double lat0, double dlat,
                                        const double *fault, double H, int crop_flag, double crop_value,
                                        void *d_state1, double *d_eta_initial, void *stream)
 {
+    // the size first, before anything touches the device
+    if (nx > 0 && ny > 0 && (long long)nx * ny > (long long)THY_OKADA_NOALLOC_MAX_CELLS) return THY_ERR_TOO_LARGE;
     int rc = check_okada_args(nx, ny, fault, crop_flag, d_state1);
     if (rc) return rc;
-    if ((long long)nx * ny > (long long)THY_OKADA_NOALLOC_MAX_CELLS) return THY_ERR_TOO_LARGE;
     int dev = 0;
     THY_CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 64) return THY_ERR_INVALID;
+    // the context the work will run in (none yet before the runtime's first
+    // use of the device: the look-up below creates it)
+    CtxGetCurrentFn get_ctx = ctx_get_current_fn();
+    if (!get_ctx) return THY_ERR_CUDA;
+    CUcontext ctx = nullptr;
+    if (get_ctx(&ctx) != CUDA_SUCCESS) return THY_ERR_CUDA;
     double *def;
     unsigned int *mx;
     {
         std::lock_guard<std::mutex> lock(g_scratch_mu);
-        if (!g_scratch_dev[dev]) {
-            void *a = nullptr, *b = nullptr;
-            THY_CK(cudaGetSymbolAddress(&a, g_okada_scratch));
-            THY_CK(cudaGetSymbolAddress(&b, g_okada_scratch_max));
-            g_scratch_dev[dev] = (double *)a;
-            g_max_dev[dev] = (unsigned int *)b;
+        ScratchAddr &a = g_scratch[dev];
+        if (!ctx || a.ctx != ctx || !a.def || !a.max) {
+            void *pd = nullptr, *pm = nullptr;
+            THY_CK(cudaGetSymbolAddress(&pd, g_okada_scratch));
+            THY_CK(cudaGetSymbolAddress(&pm, g_okada_scratch_max));
+            if (!ctx && (get_ctx(&ctx) != CUDA_SUCCESS || !ctx)) return THY_ERR_CUDA;
+            a.ctx = ctx;
+            a.def = (double *)pd;
+            a.max = (unsigned int *)pm;
         }
-        def = g_scratch_dev[dev];
-        mx = g_max_dev[dev];
+        def = a.def;
+        mx = a.max;
     }
     return enqueue_okada_reference_layout(nx, ny, lon0, dlon, lat0, dlat, fault, H, crop_flag, crop_value,
-                                          (double2 *)d_state1, d_eta_initial, def, mx, (cudaStream_t)stream);
+                                          (double2 *)d_state1, d_eta_initial, def, THY_OKADA_NOALLOC_MAX_CELLS, mx,
+                                          (cudaStream_t)stream);
 }

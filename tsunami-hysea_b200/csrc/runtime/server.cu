@@ -292,7 +292,13 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
         if ((rc = S->b.reset_lists())) return rc;
     }
     if (any_running) {
-        if ((rc = S->b.run_chunk(true))) return rc;
+        // no longer than the steps the first stepped scenario has left
+        // before an event or its end, so that it is handled (and a finished
+        // one retired, its slot and memory free) without idle launches
+        long long horizon = S->b.chunk;
+        for (int i = 0; i < cap; i++)
+            if (S->slots[i] && sel[i]) horizon = std::min(horizon, Batch::steps_to_event(*S->slots[i]->s));
+        if ((rc = S->b.run_chunk(true, S->b.chunk_for(horizon)))) return rc;
         S->stats.chunks++;
         // retire what finished in this chunk right away
         for (int i = 0; i < cap; i++) {

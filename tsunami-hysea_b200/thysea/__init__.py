@@ -206,7 +206,9 @@ def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = Tru
                nsnaps=st.snapshots, nseries=st.series_samples, tiles=st.tiles, deep_tiles=st.deep_tiles,
                dry_tiles=st.dry_tiles, setup_seconds=st.setup_seconds, output_seconds=st.output_seconds,
                total_seconds=st.total_seconds, tiling=(st.tiling.deep1, st.tiling.deep2, st.tiling.general),
-               tune_samples=st.tune_samples, release_seconds=st.release_seconds)
+               tune_samples=st.tune_samples, release_seconds=st.release_seconds, chunks=st.chunks,
+               graph_captures=st.graph_captures, capture_seconds=st.capture_seconds,
+               event_seconds=st.event_seconds, initial_seconds=st.initial_seconds)
     return res
 
 

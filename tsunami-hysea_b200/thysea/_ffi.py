@@ -74,6 +74,8 @@ class Stats(ctypes.Structure):
         ("tiles", ctypes.c_longlong), ("deep_tiles", ctypes.c_longlong), ("dry_tiles", ctypes.c_longlong),
         ("setup_seconds", ctypes.c_double), ("output_seconds", ctypes.c_double), ("total_seconds", ctypes.c_double),
         ("tiling", Tiling), ("tune_samples", ctypes.c_longlong), ("release_seconds", ctypes.c_double),
+        ("chunks", ctypes.c_longlong), ("graph_captures", ctypes.c_longlong), ("capture_seconds", ctypes.c_double),
+        ("event_seconds", ctypes.c_double), ("initial_seconds", ctypes.c_double),
     ]
 
 
@@ -165,3 +167,18 @@ def lib() -> ctypes.CDLL:
             fn.restype = res
         _lib = L
     return _lib
+
+
+_nclite = None
+
+
+def nclite() -> ctypes.CDLL:
+    """Loads libnclite.so, the library's NetCDF classic reader / writer with
+    the NetCDF C API (nc_*) exported; libthysea.so keeps its own copy private."""
+    global _nclite
+    if _nclite is None:
+        path = os.path.join(os.path.dirname(LIB_PATH), "libnclite.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"libnclite.so not built: {path} (run `python tsunami-hysea_b200/build.py`)")
+        _nclite = ctypes.CDLL(path)
+    return _nclite
