@@ -107,7 +107,7 @@ class ClockSampler:
     REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
                ("sw_power_cap", 0x4), ("hw_power_brake_slowdown", 0x80))
 
-    def __init__(self, device: int, period: float = 0.002):
+    def __init__(self, device: int, period: float = 0.0005):
         self.device = device
         self.period = period
         self.thread = None
@@ -384,20 +384,88 @@ def _pct(xs, q):
     return float(np.percentile(np.asarray(xs, dtype=np.float64), q)) if len(xs) else None
 
 
-def _plain_service(preps, out_fields):
+def _plain_service(preps, out_fields, keep=None):
     """One-at-a-time path: thy_run per scenario (an iterable of Prepared,
     made lazily by the caller if it likes), back to back; returns the service
-    time of each (s) and the cell updates."""
+    time of each (s), the cell updates and the step counts.  keep(k): whether
+    to keep a copy of scenario k's max-height field (copied after its timing)
+    for the comparison with the reference CUDA build."""
     import thysea
 
-    times, cu = [], 0.0
-    for prep in preps:
+    times, cu, steps, kept = [], 0.0, [], {}
+    for k, prep in enumerate(preps):
         out = out_fields(prep)   # (page-locked once per grid size, outside the timing)
         t0 = time.perf_counter()
         r = thysea.run(prep, snapshots=False, series=False, out=out)
         times.append(time.perf_counter() - t0)
         cu += float(prep.c.nx) * float(prep.c.ny) * float(r["iterations"])
-    return times, cu
+        steps.append(int(r["iterations"]))
+        if keep is not None and keep(k):
+            kept[k] = out["max_height"].copy()
+    return times, cu, steps, kept
+
+
+REFGPU = os.path.join(ROOT, "oracle", "_ref", "TsunamiHySEA_refgpu")
+
+
+def _rel_l2_wet(a, b):
+    """relative L2 of max-height a against b over the cells wet in both (-9999: never wet)"""
+    import numpy as np
+
+    m = (a != -9999.0) & (b != -9999.0)
+    ref = b[m].astype(np.float64)
+    den = float(np.sqrt((ref ** 2).sum()))
+    num = float(np.sqrt(((a[m].astype(np.float64) - ref) ** 2).sum()))
+    return num / den if den > 0 else num
+
+
+def _ref_cuda_service(probs, ours, sample=1, tol=1e-4):
+    """The reference CUDA build one scenario per process, back to back: the
+    reference's own path, whose main() runs one shallowWater() per run
+    (src/ShallowWater.cxx:146-151).  Each problem's files are written before
+    its clock starts; the service time is the process's wall time (CUDA
+    start-up, file input, Okada, the loop, the NetCDF output).  Every
+    `sample`-th scenario runs; each result's
+    maximum height is compared with this library's result for the same
+    scenario (ours[k]).  The reference writes its output file only when
+    saving is on (src/GPU/ShallowWater.cu:313,456), so it runs with a saving
+    interval of twice the simulated time: one snapshot at t = 0, then the
+    maximum height and arrival times at the end.  Returns per sampled
+    scenario: index, service time, the reference's own loop time,
+    iterations, max-height relative L2."""
+    import copy
+    import shutil
+
+    from scipy.io import netcdf_file
+
+    from thysea import synth
+
+    out = []
+    for k, p in enumerate(probs):
+        if k % sample:
+            continue
+        d = tempfile.mkdtemp(prefix="thy_refcuda_")
+        try:
+            q = copy.copy(p)
+            q.save_time = 2.0 * p.sim_time
+            txt = synth.write_problem(q, d)
+            t0 = time.perf_counter()
+            r = subprocess.run([REFGPU, txt], cwd=d, capture_output=True, text=True, timeout=1800)
+            wall = time.perf_counter() - t0
+            if r.returncode != 0:
+                raise RuntimeError(f"reference CUDA build failed on {p.name}: {r.stdout[-500:]} {r.stderr[-500:]}")
+            import re
+
+            runtime = float(re.findall(r"Runtime: ([0-9.eE+-]+) sec", r.stdout)[-1])
+            its = re.findall(r"Iteration\s+(\d+),", r.stdout)
+            with netcdf_file(os.path.join(d, p.name + ".nc"), "r", mmap=False) as f:
+                maxh = f.variables["max_height"][:].copy()
+            err = _rel_l2_wet(ours[k], maxh) if k in ours else None
+            out.append({"k": k, "service_s": wall, "runtime_s": runtime, "iterations": int(its[-1]) if its else None,
+                        "max_height_rel_l2": err, "ok": (err is not None and err <= tol)})
+        finally:
+            shutil.rmtree(d, ignore_errors=True)
+    return out
 
 
 def _fifo(arrivals, service):
@@ -470,9 +538,28 @@ def run_batched(a, dist):
         ttr = [r["done_at"] - t0 for r in res]
         cu = sum(c * r["stats"]["steps"] for c, r in zip(cells, res))
         # plain: one thy_run per scenario
-        p_times, p_cu = _plain_service(preps, out_fields)
+        p_times, p_cu, p_steps, ours = _plain_service(preps, out_fields, keep=lambda k: a.ref_arm)
         p_wall = sum(p_times)
         p_ttr = list(np.cumsum(p_times))
+        ref = None
+        if a.ref_arm:
+            if not os.path.exists(REFGPU):
+                ref = {"unavailable": "oracle/_ref/TsunamiHySEA_refgpu not built (reference tree absent at build)"}
+            else:
+                rr = _ref_cuda_service(probs, ours, sample=1)
+                r_wall = sum(x["service_s"] for x in rr)
+                r_ttr = list(np.cumsum([x["service_s"] for x in rr]))
+                errs = [x["max_height_rel_l2"] for x in rr if x["max_height_rel_l2"] is not None]
+                ref = {"path": "reference CUDA build, one process per scenario, back to back (one snapshot at t = 0)",
+                       "scenarios_per_hour": round(len(rr) / r_wall * 3600.0, 1), "wall_s": round(r_wall, 3),
+                       "loop_s_total": round(sum(x["runtime_s"] for x in rr), 3),
+                       "cell_updates_per_s": round(sum(c * (x["iterations"] or 0) for c, x in zip(cells, rr)) / r_wall, 1),
+                       "time_to_result_p50_s": round(_pct(r_ttr, 50), 3),
+                       "time_to_result_p99_s": round(_pct(r_ttr, 99), 3),
+                       "max_height_rel_l2_max": max(errs) if errs else None,
+                       "results_within_1e-4": sum(1 for x in rr if x["ok"]), "results": len(rr),
+                       "iterations_equal": sum(1 for x, st in zip(rr, p_steps) if x["iterations"] == st)}
+        del ours
         line = {
             "metric": "scenarios/hour", "value": round(len(probs) / wall * 3600.0, 1), "unit": "scenarios/h",
             "n_gpus": dist.world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
@@ -486,7 +573,11 @@ def run_batched(a, dist):
                       "cell_updates_per_s": round(p_cu / p_wall, 1),
                       "time_to_result_p50_s": round(_pct(p_ttr, 50), 3),
                       "time_to_result_p99_s": round(_pct(p_ttr, 99), 3)},
+            "reference_cuda": ref,
         }
+        if ref and "scenarios_per_hour" in ref:
+            line["batched_over_reference_cuda"] = round(line["value"] / ref["scenarios_per_hour"], 2)
+            line["batched_over_plain"] = round(line["value"] / line["plain"]["scenarios_per_hour"], 2)
         return line
 
     # ---- serving ----
@@ -508,15 +599,17 @@ def run_batched(a, dist):
     for n in set(sides):
         pinned_cache[(n, n)] = thysea.PinnedOutputs(shape=(n, n))   # before the clock
 
-    def make(k):
+    def make_problem(k):
         n = sides[k]
         lon, lat, z = bathy[n]
         rr = np.random.default_rng(int(seeds[k]))
-        p = synth.Problem(name=f"req{k:04d}", lon=lon, lat=lat, z=z, faults=[synth.random_fault(lon, lat, z, rr)],
-                          sim_time=float(t_sim[k]))
+        return synth.Problem(name=f"req{k:04d}", lon=lon, lat=lat, z=z, faults=[synth.random_fault(lon, lat, z, rr)],
+                             sim_time=float(t_sim[k]))
+
+    def make(k):
         # not page-locked: registering hundreds of MB from the preparing
         # threads would hold the driver while the stepping loop issues work
-        return thysea.Prepared(p)
+        return thysea.Prepared(make_problem(k))
 
     lead = 4.0   # seconds of look-ahead for the preparing threads
     pool = cf.ThreadPoolExecutor(max_workers=4)
@@ -550,9 +643,42 @@ def run_batched(a, dist):
         by_side.setdefault(sides[k], []).append(res[k]["done_at"] - t0 - arrivals[k])
     cu = sum(float(sides[k]) ** 2 * res[k]["stats"]["steps"] for k in res)
     # plain path: measured service times of the same requests, FIFO over the same arrivals
-    p_times, p_cu = _plain_service((make(k) for k in range(len(arrivals))), out_fields)
+    ref_every = max(1, a.ref_sample)
+    p_times, p_cu, p_steps, ours = _plain_service((make(k) for k in range(len(arrivals))), out_fields,
+                                                  keep=lambda k: a.ref_arm and k % ref_every == 0)
     p_ttr, p_end = _fifo(list(arrivals), p_times)
-    return {
+    ref = None
+    if a.ref_arm:
+        if not os.path.exists(REFGPU):
+            ref = {"unavailable": "oracle/_ref/TsunamiHySEA_refgpu not built (reference tree absent at build)"}
+        else:
+            # the reference CUDA build on every ref_every-th request (all of
+            # them with --ref-sample 1); the others' service times are
+            # modelled from those, as a + b x cell-updates (least squares; the
+            # step counts are this library's, equal to the reference's where
+            # both ran), and the stream is served FIFO over the same arrivals
+            rr = _ref_cuda_service([make_problem(k) if k % ref_every == 0 else None for k in range(len(arrivals))],
+                                   ours, sample=ref_every)
+            cu_k = [float(sides[k]) ** 2 * p_steps[k] for k in range(len(arrivals))]
+            xs = np.array([cu_k[x["k"]] for x in rr])
+            ys = np.array([x["service_s"] for x in rr])
+            A = np.stack([np.ones_like(xs), xs], axis=1)
+            coef = np.linalg.lstsq(A, ys, rcond=None)[0] if len(rr) >= 2 else np.array([ys.mean(), 0.0])
+            measured = {x["k"]: x["service_s"] for x in rr}
+            r_times = [measured.get(k, float(coef[0] + coef[1] * cu_k[k])) for k in range(len(arrivals))]
+            r_ttr, r_end = _fifo(list(arrivals), r_times)
+            errs = [x["max_height_rel_l2"] for x in rr if x["max_height_rel_l2"] is not None]
+            ref = {"path": "reference CUDA build, one process per request, FIFO (one snapshot at t = 0)",
+                   "measured_requests": len(rr), "modelled_requests": len(arrivals) - len(rr),
+                   "service_model_s": [round(float(coef[0]), 4), float(coef[1])],
+                   "scenarios_per_hour": round(len(arrivals) / r_end * 3600.0, 1),
+                   "time_to_result_p50_s": round(_pct(r_ttr, 50), 3),
+                   "time_to_result_p99_s": round(_pct(r_ttr, 99), 3),
+                   "service_s_total": round(sum(r_times), 3),
+                   "max_height_rel_l2_max": max(errs) if errs else None,
+                   "results_within_1e-4": sum(1 for x in rr if x["ok"]), "results": len(rr)}
+    del ours
+    line = {
         "metric": "scenarios/hour", "value": round(len(res) / wall * 3600.0, 1), "unit": "scenarios/h",
         "n_gpus": dist.world, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded)",
@@ -567,7 +693,11 @@ def run_batched(a, dist):
                   "time_to_result_p50_s": round(_pct(p_ttr, 50), 3),
                   "time_to_result_p99_s": round(_pct(p_ttr, 99), 3),
                   "service_s_total": round(sum(p_times), 3), "cell_updates_per_s": round(p_cu / sum(p_times), 1)},
+        "reference_cuda": ref,
     }
+    if ref and "scenarios_per_hour" in ref:
+        line["batched_over_reference_cuda_p99"] = round(ref["time_to_result_p99_s"] / line["time_to_result_p99_s"], 2)
+    return line
 
 
 def run_tilings(a, dist):
@@ -644,6 +774,10 @@ def main():
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
     ap.add_argument("--budget-gb", type=float, default=150.0, help="batch / mixed / serving: HBM budget")
     ap.add_argument("--tiling-rounds", type=int, default=4, help="tilings: round-robin rounds")
+    ap.add_argument("--ref-arm", type=int, default=1,
+                    help="batch / mixed / serving: also run the reference CUDA build one scenario per process (1) or not (0)")
+    ap.add_argument("--ref-sample", type=int, default=10,
+                    help="serving: the reference CUDA build runs every n-th request (1: all), the rest modelled")
     a = ap.parse_args()
     a.warmup = max(a.warmup, 3)
     dist = Dist()

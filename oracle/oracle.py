@@ -68,6 +68,18 @@ def oracle_lib():
         _lib.thy_oracle_run.argtypes = [ctypes.POINTER(_Problem), ctypes.POINTER(_Result)]
         _lib.thy_oracle_run.restype = ctypes.c_int
         _lib.thy_oracle_okada_points.argtypes = [ctypes.c_int, _f64p, _f64p, _f64p, _f64p]
+        _lib.thy_oracle_slab_open.argtypes = [ctypes.POINTER(_Problem), ctypes.c_int, ctypes.c_int]
+        _lib.thy_oracle_slab_open.restype = ctypes.c_void_p
+        _lib.thy_oracle_slab_initial_dt.argtypes = [ctypes.c_void_p]
+        _lib.thy_oracle_slab_initial_dt.restype = ctypes.c_double
+        _lib.thy_oracle_slab_apply_fault.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        _lib.thy_oracle_slab_phase1.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_double]
+        _lib.thy_oracle_slab_phase2.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        _lib.thy_oracle_slab_phase2.restype = ctypes.c_double
+        _lib.thy_oracle_slab_field.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        _lib.thy_oracle_slab_field.restype = _f64p
+        _lib.thy_oracle_slab_scales.argtypes = [ctypes.c_void_p, _f64p]
+        _lib.thy_oracle_slab_close.argtypes = [ctypes.c_void_p]
     return _lib
 
 
@@ -126,6 +138,116 @@ def _ptr(a: Optional[np.ndarray], ctype):
     if a is None:
         return ctypes.cast(None, ctype)
     return a.ctypes.data_as(ctype)
+
+
+def _problem_struct(p, max_iterations: int = -1, threads: int = 0):
+    """The oracle's problem struct for a thysea.synth.Problem, and the arrays
+    it points to (keep them alive while it is used)."""
+    nx, ny = p.nx, p.ny
+    lon = np.ascontiguousarray(p.lon, dtype=np.float64)
+    lat = np.ascontiguousarray(p.lat, dtype=np.float64)
+    z = np.ascontiguousarray(p.z, dtype=np.float32)
+    eta_file = None if p.faults else np.ascontiguousarray(
+        np.zeros_like(z) if p.eta_init is None else p.eta_init, dtype=np.float32)
+    faults = np.ascontiguousarray(p.fault_array(), dtype=np.float64) if p.faults else None
+    pts = None if p.points is None else np.ascontiguousarray(p.points, dtype=np.float64)
+    pr = _Problem()
+    pr.nx, pr.ny = nx, ny
+    pr.lon, pr.lat, pr.z = _ptr(lon, _f64p), _ptr(lat, _f64p), _ptr(z, _f32p)
+    pr.eta_file = _ptr(eta_file, _f32p)
+    pr.nfaults = len(p.faults)
+    pr.faults = _ptr(faults, _f64p)
+    pr.crop_flag, pr.crop_value = int(p.crop_flag), float(p.crop_value)
+    for i in range(4):
+        pr.borders[i] = float(p.borders[i])
+    pr.sim_time, pr.save_time = float(p.sim_time), float(p.save_time)
+    pr.series_time = float(p.series_time) if pts is not None else -1.0
+    pr.npoints = 0 if pts is None else len(pts)
+    pr.points = _ptr(pts, _f64p)
+    pr.cfl, pr.eps_h, pr.hpos, pr.stability = p.cfl, p.eps_h, p.hpos, p.stability
+    pr.manning, pr.vmax, pr.L, pr.H, pr.dif_at = p.manning, p.vmax, p.L, p.H, p.dif_at
+    pr.max_iterations = max_iterations
+    pr.threads = threads
+    return pr, [lon, lat, z, eta_file, faults, pts]
+
+
+class OracleSlab:
+    """The oracle stepping only rows [row_lo, row_hi) of its copy of the grid
+    (thy_oracle_slab_*): the building block of the row-slab decomposition
+    test.  The caller exchanges the two halo rows above and below after each
+    phase and takes the minimum next dt over all slabs."""
+
+    FIELDS = ("h", "qx", "qy", "eta_max", "t_arr", "dep")
+
+    def __init__(self, p, row_lo: int, row_hi: int, threads: int = 1):
+        lib = oracle_lib()
+        self.p = p
+        self.pr, self._keep = _problem_struct(p, threads=threads)
+        self.h = lib.thy_oracle_slab_open(ctypes.byref(self.pr), row_lo, row_hi)
+        if not self.h:
+            raise RuntimeError("thy_oracle_slab_open failed")
+        self.row_lo, self.row_hi = row_lo, row_hi
+        sc = (ctypes.c_double * 3)()
+        lib.thy_oracle_slab_scales(self.h, sc)
+        self.Ts, self.Hs, self.Hmin = sc[0], sc[1], sc[2]
+
+    def field(self, name: str) -> np.ndarray:
+        """the whole-grid array (ny, nx), a view of the oracle's memory"""
+        ptr = oracle_lib().thy_oracle_slab_field(self.h, self.FIELDS.index(name))
+        return np.ctypeslib.as_array(ptr, (self.p.ny, self.p.nx))
+
+    def initial_dt(self) -> float:
+        return float(oracle_lib().thy_oracle_slab_initial_dt(self.h))
+
+    def apply_fault(self, k: int):
+        oracle_lib().thy_oracle_slab_apply_fault(self.h, k)
+
+    def phase1(self, t: float, dt: float):
+        oracle_lib().thy_oracle_slab_phase1(self.h, t, dt)
+
+    def phase2(self, dt: float) -> float:
+        return float(oracle_lib().thy_oracle_slab_phase2(self.h, dt))
+
+    def close(self):
+        if self.h:
+            oracle_lib().thy_oracle_slab_close(self.h)
+            self.h = None
+
+
+def slab_rows(ny: int, rank: int, world: int):
+    """rows [lo, hi) of rank `rank` in an even row-slab split of ny rows"""
+    return ny * rank // world, ny * (rank + 1) // world
+
+
+def run_slabs(p, rank: int, world: int, steps: int, exchange, allreduce_min, threads: int = 1):
+    """Steps problem p for `steps` steps as rank `rank` of `world` row slabs.
+    exchange(name, arr, lo, hi): makes rows lo-2, lo-1 and hi, hi+1 of the
+    whole-grid array `arr` (those that exist) the neighbouring ranks' values;
+    allreduce_min(v): the minimum over ranks.  Faults are applied at their
+    times as the single-process loop does (all of them at t = 0 here: no dt
+    truncation to later fault times).  Returns the slab object."""
+    lo, hi = slab_rows(p.ny, rank, world)
+    s = OracleSlab(p, lo, hi, threads=threads)
+    tf = [f.time for f in p.faults]
+    if any(t > 0.0 for t in tf):
+        raise ValueError("run_slabs: faults at t = 0 only")
+    dt = allreduce_min(s.initial_dt())
+    t = 0.0
+    fidx = 0
+    for _ in range(steps):
+        while fidx < len(tf) and t * s.Ts >= tf[fidx]:
+            s.apply_fault(fidx)
+            fidx += 1
+        s.phase1(t, dt)
+        exchange("h", s.field("h"), lo, hi)
+        local = s.phase2(dt)
+        exchange("qx", s.field("qx"), lo, hi)
+        exchange("qy", s.field("qy"), lo, hi)
+        nxt = allreduce_min(local)
+        t += dt
+        dt = nxt
+    s.t = t
+    return s
 
 
 def run_oracle(p, max_iterations: int = -1, threads: int = 0, max_snaps: int = 0, max_series: int = 0) -> Dict:

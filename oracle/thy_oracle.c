@@ -54,6 +54,9 @@ typedef struct {
     double *acc_m, *acc_l, *acc_qx, *acc_qy;  /* accumulators: mass, lambda*len, momenta */
     double *dtc;                              /* per-cell dt */
     double *eta_max, *t_arr, *eta_ini;
+    int row_lo, row_hi;                       /* rows this process updates: [row_lo, row_hi) (all of them in
+                                                 a single-process run; a row slab in a decomposed run, whose
+                                                 two rows above and below are halos kept current by the caller) */
 } grid_t;
 
 /* src/GPU/Arista_kernel.cu:6-21 — x index with periodic wrap or clamp */
@@ -612,7 +615,7 @@ static void x_edge_pass(grid_t *g, int parity, pass_t kind, double dt)
 {
     int y;
 #pragma omp parallel for schedule(static)
-    for (y = 0; y < g->ny; y++) {
+    for (y = g->row_lo; y < g->row_hi; y++) {
         int x;
         for (x = parity; x <= g->nx; x += 2) {
             edge_t e;
@@ -631,6 +634,7 @@ static void y_edge_pass(grid_t *g, int parity, pass_t kind, double dt)
 #pragma omp parallel for schedule(static)
     for (y = parity; y <= g->ny; y += 2) {
         int x;
+        if (y < g->row_lo || y > g->row_hi) continue;   /* touches no row this process updates */
         for (x = 0; x < g->nx; x++) {
             edge_t e;
             gather_y_edge(g, x, y, &e);
@@ -659,7 +663,7 @@ static void update_mass(grid_t *g, double dt)
     int y;
     const int any_sponge = g->sp_left > 0 || g->sp_right > 0 || g->sp_up > 0 || g->sp_low > 0;
 #pragma omp parallel for schedule(static)
-    for (y = 0; y < g->ny; y++) {
+    for (y = g->row_lo; y < g->row_hi; y++) {
         int x;
         double val = dt / g->area[y];
         for (x = 0; x < g->nx; x++) {
@@ -698,7 +702,7 @@ static double update_momentum(grid_t *g, double dt)
     double dtmin = 1e300;
     const int any_sponge = g->sp_left > 0 || g->sp_right > 0 || g->sp_up > 0 || g->sp_low > 0;
 #pragma omp parallel for schedule(static) reduction(min : dtmin)
-    for (y = 0; y < g->ny; y++) {
+    for (y = g->row_lo; y < g->row_hi; y++) {
         int x;
         double area = g->area[y], val = dt / area;
         for (x = 0; x < g->nx; x++) {
@@ -782,7 +786,7 @@ static double initial_dt(grid_t *g)
     float cfl_f = (float)g->cfl;
     memset(g->acc_l, 0, sizeof(double) * g->n);
     all_edges(g, PASS_INITIAL, 0.0);
-    for (i = 0; i < g->n; i++) {
+    for (i = (long long)g->row_lo * g->nx; i < (long long)g->row_hi * g->nx; i++) {
         int y = (int)(i / g->nx);
         double area = g->area[y];
         double s = (g->acc_l[i] < EPS) ? 1e30 : (2.0 * cfl_f * area) / g->acc_l[i];
@@ -1030,30 +1034,28 @@ static void free_grid(grid_t *g)
     free(g->eta_max); free(g->t_arr); free(g->eta_ini);
 }
 
-int thy_oracle_run(const thy_oracle_problem *p, thy_oracle_result *r)
+/* The problem loader's set-up (src/Problema.cxx:319-448): scales,
+ * dimensionless parameters, arrays, bathymetry with the Hmin shift, metric
+ * terms and the initial state (Okada-style or from the initial-state file).
+ * Returns 0, 1 (bad size) or 2 (no memory). */
+static int grid_setup(grid_t *gp, const thy_oracle_problem *p)
 {
-    grid_t g;
-    int nx = p->nx, ny = p->ny, i, nf = p->nfaults, fidx = 0, jumping = 0, snaps = 0, series = 0;
-    long long n = (long long)nx * ny, c, iter;
-    double *faults = NULL, *tfault = NULL, R_nd, tend, save_nc, save_ts, t = 0.0, dt, next_nc = 0.0, next_ts = 0.0;
-    int *gpos = NULL, ngauge = 0;
-    double *glon = NULL, *glat = NULL;
-    struct timespec ts0, ts1;
+#define g (*gp)
+    int nx = p->nx, ny = p->ny, i;
+    long long n = (long long)nx * ny, c;
+    double R_nd;
     const double g2r = M_PI / 180.0;
-
     if (nx < 2 || ny < 2) return 1;
 #ifdef _OPENMP
     if (p->threads > 0) omp_set_num_threads(p->threads);
 #endif
     memset(&g, 0, sizeof(g));
     g.nx = nx; g.ny = ny; g.n = n;
+    g.row_lo = 0; g.row_hi = ny;
     /* scales and dimensionless parameters (src/Problema.cxx:319-349) */
     g.Ls = p->L; g.Hs = p->H;
     g.Qs = sqrt(9.81 * pow(g.Hs, 3.0));
     g.Ts = g.Ls * g.Hs / g.Qs;
-    tend = p->sim_time / g.Ts;
-    save_nc = p->save_time / g.Ts;
-    save_ts = p->series_time / g.Ts;
     g.mf0 = p->manning * (9.81 * p->manning * g.Ls / pow(g.Hs, 4.0 / 3.0));
     g.vmax = p->vmax / (g.Qs / g.Hs);
     g.eps_h = p->eps_h / g.Hs;
@@ -1116,6 +1118,24 @@ int thy_oracle_run(const thy_oracle_problem *p, thy_oracle_result *r)
             g.h[c] = dmax(v, 0.0);
         }
     }
+    return 0;
+#undef g
+}
+
+int thy_oracle_run(const thy_oracle_problem *p, thy_oracle_result *r)
+{
+    grid_t g;
+    int nx = p->nx, ny = p->ny, i, nf = p->nfaults, fidx = 0, jumping = 0, snaps = 0, series = 0, rc;
+    long long n = (long long)nx * ny, c, iter;
+    double *faults = NULL, *tfault = NULL, tend, save_nc, save_ts, t = 0.0, dt, next_nc = 0.0, next_ts = 0.0;
+    int *gpos = NULL, ngauge = 0;
+    double *glon = NULL, *glat = NULL;
+    struct timespec ts0, ts1;
+
+    if ((rc = grid_setup(&g, p))) return rc;
+    tend = p->sim_time / g.Ts;
+    save_nc = p->save_time / g.Ts;
+    save_ts = p->series_time / g.Ts;
     /* faults sorted by time (src/Problema.cxx:97-126, selection sort) */
     if (nf > 0) {
         faults = malloc(sizeof(double) * 10 * nf);
@@ -1251,4 +1271,109 @@ int thy_oracle_run(const thy_oracle_problem *p, thy_oracle_result *r)
     free_grid(&g);
     (void)zero_acc;
     return 0;
+}
+
+/* ---------------------------------------------------------------------- */
+/* Row slabs: the same stepper on a process that updates only rows         */
+/* [row_lo, row_hi) of the grid.  The caller keeps the two rows above and   */
+/* below the slab current (halo exchange) after each phase, and takes the   */
+/* minimum of every process's next dt; then each updated cell sees exactly  */
+/* the values it would see in a single-process run (the stencil reaches two */
+/* rows), so the decomposed run gives bitwise the same state.               */
+/* ---------------------------------------------------------------------- */
+
+struct thy_oracle_slab {
+    grid_t g;
+    const thy_oracle_problem *p;
+    double *def;
+};
+
+thy_oracle_slab *thy_oracle_slab_open(const thy_oracle_problem *p, int row_lo, int row_hi)
+{
+    long long c;
+    thy_oracle_slab *s;
+    if (row_lo < 0 || row_hi > p->ny || row_lo >= row_hi) return NULL;
+    s = calloc(1, sizeof(*s));
+    if (!s) return NULL;
+    if (grid_setup(&s->g, p)) {
+        free(s);
+        return NULL;
+    }
+    s->p = p;
+    s->g.row_lo = row_lo;
+    s->g.row_hi = row_hi;
+    /* metrics initialised on the pre-deformation state (src/GPU/ShallowWater.cu:305-309) */
+    for (c = 0; c < s->g.n; c++) {
+        s->g.eta_max[c] = (s->g.h[c] < s->g.eps_h) ? -1e30 : s->g.h[c] - s->g.dep[c];
+        s->g.eta_ini[c] = s->g.eta_max[c];
+        s->g.t_arr[c] = -1.0;
+    }
+    s->def = malloc(sizeof(double) * s->g.n);
+    if (!s->def) {
+        thy_oracle_slab_close(s);
+        return NULL;
+    }
+    return s;
+}
+
+double thy_oracle_slab_initial_dt(thy_oracle_slab *s) { return initial_dt(&s->g); }
+
+void thy_oracle_slab_apply_fault(thy_oracle_slab *s, int k)
+{
+    const thy_oracle_problem *p = s->p;
+    apply_fault(&s->g, p->faults + 10 * k, p->lon, p->lat, p->crop_flag,
+                p->crop_flag == 2 ? p->crop_value / s->g.Hs : p->crop_value, s->def);
+}
+
+void thy_oracle_slab_phase1(thy_oracle_slab *s, double t, double dt)
+{
+    grid_t *g = &s->g;
+    long long c;
+    /* metrics of the state the step starts from (src/GPU/Metrics.cu:23-77) */
+    for (c = (long long)g->row_lo * g->nx; c < (long long)g->row_hi * g->nx; c++) {
+        double e = g->h[c] - g->dep[c];
+        if (e > g->eta_max[c] && g->h[c] > g->eps_h) g->eta_max[c] = e;
+        if (g->t_arr[c] < 0.0 && fabs(e - g->eta_ini[c]) > g->dif_at) g->t_arr[c] = t;
+    }
+    memset(g->acc_m, 0, sizeof(double) * g->n);
+    all_edges(g, PASS_MASS, dt);
+    update_mass(g, dt);
+}
+
+double thy_oracle_slab_phase2(thy_oracle_slab *s, double dt)
+{
+    grid_t *g = &s->g;
+    memset(g->acc_l, 0, sizeof(double) * g->n);
+    memset(g->acc_qx, 0, sizeof(double) * g->n);
+    memset(g->acc_qy, 0, sizeof(double) * g->n);
+    all_edges(g, PASS_MOMENTUM, dt);
+    return update_momentum(g, dt);
+}
+
+double *thy_oracle_slab_field(thy_oracle_slab *s, int which)
+{
+    switch (which) {
+    case 0: return s->g.h;
+    case 1: return s->g.qx;
+    case 2: return s->g.qy;
+    case 3: return s->g.eta_max;
+    case 4: return s->g.t_arr;
+    case 5: return s->g.dep;
+    default: return NULL;
+    }
+}
+
+void thy_oracle_slab_scales(const thy_oracle_slab *s, double *ts_hs_hmin)
+{
+    ts_hs_hmin[0] = s->g.Ts;
+    ts_hs_hmin[1] = s->g.Hs;
+    ts_hs_hmin[2] = s->g.Hmin;
+}
+
+void thy_oracle_slab_close(thy_oracle_slab *s)
+{
+    if (!s) return;
+    free(s->def);
+    free_grid(&s->g);
+    free(s);
 }

@@ -63,6 +63,24 @@ int thy_oracle_run(const thy_oracle_problem *p, thy_oracle_result *r);
  * fault (10 values as in thy_oracle_problem.faults). */
 void thy_oracle_okada_points(int n, const double *lon, const double *lat, const double *fault, double *uz);
 
+/* Row slabs, for the test of a row-slab decomposition of one grid: the
+ * process updates only rows [row_lo, row_hi) of its copy of the whole grid;
+ * the caller keeps the two rows above and below the slab current after each
+ * phase (h after phase 1; qx, qy after phase 2) and steps every process
+ * with the minimum of their next dt.  Faults are applied when the caller
+ * says so (thy_oracle_slab_apply_fault, fault k of the problem's list). */
+typedef struct thy_oracle_slab thy_oracle_slab;
+thy_oracle_slab *thy_oracle_slab_open(const thy_oracle_problem *p, int row_lo, int row_hi);
+double thy_oracle_slab_initial_dt(thy_oracle_slab *s);        /* minimum over the slab's rows */
+void thy_oracle_slab_apply_fault(thy_oracle_slab *s, int k);
+void thy_oracle_slab_phase1(thy_oracle_slab *s, double t, double dt);   /* metrics at t, mass update */
+double thy_oracle_slab_phase2(thy_oracle_slab *s, double dt);  /* momentum update; next dt over the slab */
+/* the whole-grid arrays (ny*nx doubles, dimensionless): 0 h, 1 qx, 2 qy,
+ * 3 eta_max, 4 arrival time, 5 shifted depth */
+double *thy_oracle_slab_field(thy_oracle_slab *s, int which);
+void thy_oracle_slab_scales(const thy_oracle_slab *s, double *ts_hs_hmin);   /* time scale, depth scale, Hmin */
+void thy_oracle_slab_close(thy_oracle_slab *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -84,13 +84,26 @@ int main(int argc, char **argv)
     } else if (!std::strcmp(sc, "keys")) {
         Costs a{{1.0, 0.5, 1.0}, {1.0, 1.0, 1.0}, {1.0, 1.0, 1.0}};
         Costs b{{1.0, 1.0, 1.0}, {1.0, 1.0, 1.0}, {1.0, 1.0, 0.5}};
-        const TuneKey k2{0, 7, 3};
+        const TuneKey k2{0, 10, 3};
         run_to_decision(k, a, 0.0, &chunks);
         print("keys-a", k, chunks);
         run_to_decision(k2, b, 0.0, &chunks);
         print("keys-b", k2, chunks);
         std::printf("bucket 1=%d 2=%d 3=%d 1024=%d 1025=%d\n", tune_bucket(1), tune_bucket(2), tune_bucket(3),
                     tune_bucket(1024), tune_bucket(1025));
+    } else if (!std::strcmp(sc, "small")) {
+        // a step of at most 512 units: the short-chain tiling, decided, no sample wanted
+        const TuneKey ks{0, 7, 8};
+        bool s = true;
+        const Tiling t = tuner_pick(ks, &s);
+        Tiling best;
+        best.deep1 = 9;
+        const bool done = tuner_decided(ks, &best);
+        std::printf("small pick=%d,%d,%d sampling=%d done=%d best=%d,%d,%d\n", t.deep1, t.deep2, t.general, s ? 1 : 0,
+                    done ? 1 : 0, best.deep1, best.deep2, best.general);
+        const TuneKey kb{0, 9, 1};   // 514 units: tuned
+        const Tiling u = tuner_pick(kb, &s);
+        std::printf("larger pick=%d,%d,%d sampling=%d\n", u.deep1, u.deep2, u.general, s ? 1 : 0);
     } else if (!std::strcmp(sc, "cache")) {
         // first process: decide and write; then forget and read back
         Costs c{{1.0, 0.5, 1.0}, {1.0, 1.0, 0.5}, {1.0, 1.0, 1.0}};

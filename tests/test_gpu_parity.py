@@ -157,3 +157,28 @@ def test_async_snapshots_and_gauges_in_order(gpu):
     ts = np.asarray(g["series"]["time"])
     assert len(ts) == g["nseries"] == r["nseries"] and np.all(np.diff(ts) > 0)
     assert np.abs(np.asarray(g["series"]["eta"]) - r["series"]["eta"]).max() <= ETA_TOL_M
+
+
+def test_gauges_sampled_on_the_device_do_not_stop_the_run(gpu):
+    """gauge times are handled by the step controller on the device: a run
+    with gauges every 10 s takes exactly the graph launches of the same run
+    without gauges, its samples are those of the oracle at the same times, and
+    the extremes of eta folded on the device are the oracle's"""
+    base = dict(nx=256, ny=192, sim_time=400.0, save_time=-1.0, npoints=8)
+    with_g = synth.plain_small(series_time=10.0, **base)
+    with_g.name = "gauges_device"
+    without = synth.plain_small(series_time=-1.0, **base)
+    without.name = "gauges_none"
+    g, r, c = _both(gpu, with_g, max_snaps=4, max_series=64)
+    _assert_parity(c, snaps=False)
+    g0 = gpu.run(without)
+    assert g["iterations"] == g0["iterations"]
+    assert g["chunks"] == g0["chunks"], (g["chunks"], g0["chunks"])
+    assert g["nseries"] == r["nseries"] and g["nseries"] >= 40
+    ts = np.asarray(g["series"]["time"])
+    assert np.all(np.diff(ts) > 0)
+    assert np.abs(ts - r["series"]["time"][:len(ts)]).max() < 1e-3
+    assert np.abs(np.asarray(g["series"]["eta"]) - r["series"]["eta"]).max() <= ETA_TOL_M
+    nu = len(r["series"]["min"])
+    assert np.abs(g["series"]["min"][:nu] - r["series"]["min"]).max() <= ETA_TOL_M
+    assert np.abs(g["series"]["max"][:nu] - r["series"]["max"]).max() <= ETA_TOL_M

@@ -50,8 +50,21 @@ def test_every_tiling_gives_the_same_results(gpu, untuned):
             assert np.array_equal(got[k], ref[k], equal_nan=True), (t, k)
 
 
+def _tuned_problem():
+    # enough work per step (640 units) for the autotuner, which leaves steps
+    # of at most 512 units at the default tiling
+    p = synth.single_large(n=1024, seed=31, sim_time=600.0)
+    p.name = "tiling_tuned"
+    return p
+
+
+def test_small_steps_run_the_short_chain_tiling_untuned(gpu, untuned):
+    r = thysea.run(thysea.Prepared(_problem()), snapshots=False, series=False)
+    assert r["tune_samples"] == 0 and r["tiling"] == (0, 2, 2)
+
+
 def test_autotuned_run_gives_the_default_results(gpu, untuned):
-    prep = thysea.Prepared(_problem())
+    prep = thysea.Prepared(_tuned_problem())
     thysea.force_tiling((0, 0, 0))
     ref, r0 = _run(prep)
     thysea.force_tiling(None)
@@ -62,7 +75,7 @@ def test_autotuned_run_gives_the_default_results(gpu, untuned):
 
 
 def test_session_tune_decides(gpu, untuned):
-    p = synth.single_large(n=640, seed=32, sim_time=3600.0)
+    p = synth.single_large(n=1024, seed=32, sim_time=3600.0)
     s = thysea.Session(p)
     steps = s.tune()
     # 3 kernels x 3 candidates x 2 samples of one 16-step chunk each, after a

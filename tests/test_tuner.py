@@ -67,6 +67,13 @@ def test_size_buckets_are_independent(driver):
     assert out[2] == "bucket 1=0 2=1 3=2 1024=10 1025=11"
 
 
+def test_small_steps_are_not_tuned(driver):
+    out = _run(driver, "small")
+    assert _field(out[0], "pick") == "0,2,2" and _field(out[0], "sampling") == "0"
+    assert _field(out[0], "done") == "1" and _field(out[0], "best") == "0,2,2"
+    assert _field(out[1], "sampling") == "1"
+
+
 def test_forced_tiling_and_environment(driver):
     out = _run(driver, "force")
     assert _field(out[0], "pick") == "2,1,2" and _field(out[0], "sampling") == "0"

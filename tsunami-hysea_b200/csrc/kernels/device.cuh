@@ -68,7 +68,13 @@ struct ScenarioCtl {
     const double *fault_times; // nfaults fault times (s), sorted, device memory
     unsigned long long units_deep;   // work units stepped by the deep-water kernels (phase 2)
     unsigned long long units_dry;    // work units skipped as dry land (classifications)
+    unsigned int gauge_count;  // gauge samples the controller took (ring slot = count % kGaugeRing)
 };
+
+// Gauge samples taken on the device between two reads by the host: at most
+// one per step, and the host reads them after every chunk of at most
+// kGaugeRing steps.
+constexpr int kGaugeRing = 32;
 
 // Opaque 128-byte TMA tensor map (CUtensorMap), 64-byte aligned in device memory.
 struct alignas(64) TmaMap {
@@ -124,7 +130,50 @@ struct ScenarioDev {
     const float4 *rowpack;
     RowMetrics row;
     ScenarioCtl *ctl;
+    // gauges (time-series points), sampled by the step controller at each
+    // gauge time that does not coincide with a fault
+    const int *gauge_cells;   // ngauges cell indices (y nx + x; -1: outside the grid)
+    int ngauges;
+    float *gauge_ring;        // kGaugeRing samples of ngauges x {eta, ux, uy, depth} (m, m/s)
+    double *gauge_ring_t;     // their times (s)
+    float2 *gauge_minmax;     // per gauge {min, max} of eta over every sample (-9999 outside the grid)
+    double Hs, Qs;            // depth and discharge scales (dimensional outputs)
 };
+
+// One gauge of the state at `parity` in dimensional units (eta, ux, uy,
+// depth: src/GPU/Volumen_kernel.cu:223-254 with the output scaling of
+// src/GPU/netcdfSeries.cu), -9999 for a point outside the grid; folds eta into
+// the gauge's {min, max} when minmax is not null (the running extremes of
+// src/GPU/netcdfSeries.cu:125,138).
+__device__ __forceinline__ void gauge_values(const ScenarioDev &s, int parity, int cell, float *out4, float2 *minmax)
+{
+    if (cell < 0) {
+        out4[0] = out4[1] = out4[2] = out4[3] = -9999.0f;
+        return;
+    }
+    const int x = cell % s.nx, y = cell / s.nx;
+    const size_t idx = (size_t)y * s.pitch + x;
+    const double eta = (double)s.eta[parity][idx], D = (double)s.dep[idx];
+    const double h = eta + D, eps_h = s.eps_h64;
+    double f;
+    if (h < eps_h) {
+        const double e4 = eps_h * eps_h * eps_h * eps_h;
+        f = 1.41421356237309505 * h / sqrt(h * h * h * h + e4);
+    } else {
+        f = 1.0 / h;
+    }
+    const float e = (float)(eta * s.Hs);
+    out4[0] = e;
+    out4[1] = (float)(f * (double)s.qx[parity][idx] * s.Qs / s.Hs);
+    out4[2] = (float)(f * (double)s.qy[parity][idx] * s.Qs / s.Hs);
+    out4[3] = (float)(D * s.Hs);
+    if (minmax) {
+        float2 m = *minmax;
+        m.x = (m.x < e) ? m.x : e;
+        m.y = (e < m.y) ? m.y : e;
+        *minmax = m;
+    }
+}
 
 __host__ __device__ inline float fmax_(float a, float b) { return (a < b) ? b : a; }
 __host__ __device__ inline float fmin_(float a, float b) { return (b < a) ? b : a; }

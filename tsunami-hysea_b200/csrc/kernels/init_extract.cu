@@ -94,38 +94,130 @@ void launch_extract(const ScenarioDev *s_host, int field, int parity, float *out
 }
 
 __global__ void gauges_kernel(ScenarioDev s, int parity, const int *__restrict__ cells, int nP, float *__restrict__ out4,
-                              double Hs, double Qs, double eps_h)
+                              float2 *__restrict__ minmax)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= nP) return;
-    const int c = cells[k];
-    if (c < 0) {
-        out4[4 * k + 0] = out4[4 * k + 1] = out4[4 * k + 2] = out4[4 * k + 3] = -9999.0f;
-        return;
-    }
-    const int x = c % s.nx, y = c / s.nx;
-    const size_t idx = (size_t)y * s.pitch + x;
-    const double eta = (double)s.eta[parity][idx], D = (double)s.dep[idx];
-    const double h = eta + D;
-    double f;
-    if (h < eps_h) {
-        const double e4 = eps_h * eps_h * eps_h * eps_h;
-        f = 1.41421356237309505 * h / sqrt(h * h * h * h + e4);
-    } else {
-        f = 1.0 / h;
-    }
-    out4[4 * k + 0] = (float)(eta * Hs);
-    out4[4 * k + 1] = (float)(f * (double)s.qx[parity][idx] * Qs / Hs);
-    out4[4 * k + 2] = (float)(f * (double)s.qy[parity][idx] * Qs / Hs);
-    out4[4 * k + 3] = (float)(D * Hs);
+    gauge_values(s, parity, cells[k], out4 + 4 * k, minmax ? minmax + k : nullptr);
 }
 
-void launch_gauges(const ScenarioDev *s_host, int parity, const int *cells, int nP, float *out4, double Hs, double Qs,
-                   double Hmin, cudaStream_t st)
+void launch_gauges(const ScenarioDev *s_host, int parity, const int *cells, int nP, float *out4, bool fold_minmax,
+                   cudaStream_t st)
 {
-    (void)Hmin;
     if (nP <= 0) return;
-    gauges_kernel<<<(nP + 127) / 128, 128, 0, st>>>(*s_host, parity, cells, nP, out4, Hs, Qs, s_host->eps_h64);
+    gauges_kernel<<<(nP + 127) / 128, 128, 0, st>>>(*s_host, parity, cells, nP, out4,
+                                                    fold_minmax ? s_host->gauge_minmax : nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// Step controller (the last launch of every step), one block per scenario
+// slot (src/GPU/ShallowWater.cu:397-450 loop body after the step;
+// src/GPU/Timestep.cu:35-68 dt truncation to fault times).  Thread 0 reads
+// the control block once (plain loads see the step's atomics), advances time
+// and dt in registers and writes the changed fields back.  At a gauge time
+// the block samples the gauges of the state the step produced into the
+// scenario's ring (the reference copies them to the host at every gauge
+// time, src/GPU/ShallowWater.cu:410-421), so that a gauge time does not stop
+// the scenario; only a gauge time that coincides with a fault pauses it (the
+// reference applies the fault first), like snapshots and faults do.  Compiled
+// without fast math, as the other output kernels, so that a gauge sample is
+// the same whether the device or the host takes it.
+// ---------------------------------------------------------------------------
+constexpr int kControllerThreads = 128;
+
+__global__ void __launch_bounds__(kControllerThreads) controller_kernel(const ScenarioDev *__restrict__ scen, int nslots)
+{
+    const ScenarioDev &s = scen[blockIdx.x];
+    __shared__ int s_sample;   // ring slot of a gauge sample taken at this step, or -1
+    __shared__ int s_parity;
+    if (threadIdx.x == 0) {
+        s_sample = -1;
+        ScenarioCtl *cp = s.ctl;
+        if (cp && cp->status == kRunning) {
+            ScenarioCtl c = *cp;
+            const float dmin = __uint_as_float(c.dt_bits);
+            const unsigned errs = c.errors;
+            c.t += c.dt;
+            double dt = (double)dmin;
+            // truncation so that t lands on the next fault time
+            const int nf = c.nfaults;
+            const int f = c.fault_next;
+            const double *tf = c.fault_times;
+            if (!c.jumping) {
+                if (f < nf && (c.t + dt) * c.T > tf[f]) {
+                    dt = tf[f] / c.T - c.t;
+                    c.jumping = 1;
+                }
+            } else {
+                c.jumping = 0;
+                if (f < nf) {
+                    int i = f + 1;
+                    while (i < nf && !(fabs(tf[i] - tf[f]) > 2.220446049250313e-16)) i++;
+                    if (i < nf && (c.t + dt) * c.T > tf[i]) {
+                        dt = tf[i] / c.T - c.t;
+                        c.jumping = 1;
+                    }
+                }
+            }
+            c.dt = dt;
+            c.step += 1;
+            c.parity ^= 1;
+            c.dt_bits = 0x7f7fffffu;
+            c.tiles_done = 0u;
+            int ev = 0;
+            if (errs || !(dmin > 0.f) || isnan(dmin)) {
+                c.status = kFailed;
+            } else if (!(c.t < c.t_end)) {
+                c.status = kDone;
+            } else if (c.max_steps >= 0 && c.step >= c.max_steps) {
+                c.events = kEvStepBudget;
+                c.status = kDone;
+            } else {
+                if (f < nf && c.t * c.T >= tf[f]) ev |= kEvFault;
+                if (c.save_nc >= 0.0 && c.t >= c.next_nc) ev |= kEvSnapshot;
+                if (c.save_ts >= 0.0 && c.t >= c.next_ts) {
+                    if (s.ngauges > 0 && !(ev & kEvFault)) {
+                        // the loop's gauge event on the device: same time test
+                        // and interval update as the host's
+                        s_sample = (int)(c.gauge_count % kGaugeRing);
+                        s.gauge_ring_t[s_sample] = c.t * c.T;
+                        c.next_ts += c.save_ts;
+                        c.gauge_count += 1;
+                    } else {
+                        ev |= kEvSeries;
+                    }
+                }
+                if (ev) {
+                    c.events = ev;
+                    c.status = kPaused;
+                }
+            }
+            cp->t = c.t;
+            cp->dt = c.dt;
+            cp->step = c.step;
+            cp->parity = c.parity;
+            cp->jumping = c.jumping;
+            cp->dt_bits = c.dt_bits;
+            cp->tiles_done = c.tiles_done;
+            cp->events = c.events;
+            cp->status = c.status;
+            cp->next_ts = c.next_ts;
+            cp->gauge_count = c.gauge_count;
+            s_parity = c.parity;
+        }
+    }
+    __syncthreads();
+    const int slot = s_sample;
+    if (slot < 0) return;
+    float *dst = s.gauge_ring + (size_t)slot * 4 * s.ngauges;
+    for (int k = threadIdx.x; k < s.ngauges; k += blockDim.x)
+        gauge_values(s, s_parity, s.gauge_cells[k], dst + 4 * k, s.gauge_minmax + k);
+    (void)nslots;
+}
+
+void launch_controller(const StepLaunch &L, cudaStream_t st)
+{
+    controller_kernel<<<L.nslots, kControllerThreads, 0, st>>>(L.scen, L.nslots);
 }
 
 }  // namespace thy

@@ -76,7 +76,8 @@ struct StepLaunch {
     const int2 *work;          // work list: (scenario slot, tile)
     const int *nwork;          // its length (device)
     int *lists;                // deep / general lists of the step: 2 counts + 2 x cap indices
-    int *claims;               // units claimed beyond the first wave by deep phase 1 / 2 (zeroed by classification)
+    int *claims;               // units claimed beyond the first wave by deep phase 1 / 2 and the general
+                               // kernel of phase 1 / 2 (zeroed by classification)
     int cap;                   // list capacity (>= work-list length)
     int grid;                  // general kernel grid
     int deep_grid[2];          // persistent deep kernel grids, phase 1 and 2
@@ -94,6 +95,8 @@ void launch_initial_dt(const StepLaunch &L, cudaStream_t st);
 // lists for the current states of the work list's scenarios (from the host,
 // before a chunk: after the work list or a state changed)
 void launch_lists_current(const StepLaunch &L, cudaStream_t st);
+// init_extract.cu: the step controller of every slot (launch 5 of a step)
+void launch_controller(const StepLaunch &L, cudaStream_t st);
 int deep_blocks_per_sm(int phase, int variant);
 
 // init.cu: double-precision host state (reference layout, dimensionless) to
@@ -116,8 +119,10 @@ void launch_apply_deformation(const ScenarioDev *s_host, const double *def, int 
 enum Field { kFieldEta = 0, kFieldUx = 1, kFieldUy = 2, kFieldMaxHeight = 3, kFieldArrival = 4, kFieldDeformed = 5 };
 void launch_extract(const ScenarioDev *s_host, int field, int parity, float *out, double Hs, double Qs, double Hmin,
                     cudaStream_t st);
-// gauges: eta (m), ux, uy (m/s) and depth at nP cells (cell index or -1)
-void launch_gauges(const ScenarioDev *s_host, int parity, const int *cells, int nP, float *out4, double Hs, double Qs,
-                   double Hmin, cudaStream_t st);
+// gauges: eta (m), ux, uy (m/s) and depth at nP cells (cell index or -1);
+// fold_minmax: a sample of the series, its eta folded into the scenario's
+// gauge extremes (not for the final read of the depths)
+void launch_gauges(const ScenarioDev *s_host, int parity, const int *cells, int nP, float *out4, bool fold_minmax,
+                   cudaStream_t st);
 
 }  // namespace thy

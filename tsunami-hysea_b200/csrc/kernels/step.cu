@@ -39,6 +39,7 @@
 #include "device.cuh"
 #include "kernels.h"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace thy {
@@ -146,73 +147,6 @@ __device__ __forceinline__ float initial_speed(Edge &e, const ScenarioDev &s)
     float maxa = fabsf(uij) + sqrtf(hij);
     if (maxa < s.eps_h) maxa += s.eps_h;
     return e.len * maxa;
-}
-
-// Step controller of one scenario, run after its phase-2 tiles
-// (src/GPU/ShallowWater.cu:397-450 loop body after the step;
-//  src/GPU/Timestep.cu:35-68 dt truncation to fault times).
-__device__ void controller(const ScenarioDev &s)
-{
-    // one thread per scenario, in its own launch after the phase-2 kernels:
-    // the control block is read once (plain loads see their atomics), updated
-    // in registers and the changed fields written back
-    ScenarioCtl *cp = s.ctl;
-    ScenarioCtl c = *cp;
-    const float dmin = __uint_as_float(c.dt_bits);
-    const unsigned errs = c.errors;
-    c.t += c.dt;
-    double dt = (double)dmin;
-    // truncation so that t lands on the next fault time
-    const int nf = c.nfaults;
-    const int f = c.fault_next;
-    const double *tf = c.fault_times;
-    if (!c.jumping) {
-        if (f < nf && (c.t + dt) * c.T > tf[f]) {
-            dt = tf[f] / c.T - c.t;
-            c.jumping = 1;
-        }
-    } else {
-        c.jumping = 0;
-        if (f < nf) {
-            int i = f + 1;
-            while (i < nf && !(fabs(tf[i] - tf[f]) > 2.220446049250313e-16)) i++;
-            if (i < nf && (c.t + dt) * c.T > tf[i]) {
-                dt = tf[i] / c.T - c.t;
-                c.jumping = 1;
-            }
-        }
-    }
-    c.dt = dt;
-    c.step += 1;
-    c.parity ^= 1;
-    c.dt_bits = 0x7f7fffffu;
-    c.tiles_done = 0u;
-    int ev = 0;
-    if (errs || !(dmin > 0.f) || isnan(dmin)) {
-        c.status = kFailed;
-    } else if (!(c.t < c.t_end)) {
-        c.status = kDone;
-    } else if (c.max_steps >= 0 && c.step >= c.max_steps) {
-        c.events = kEvStepBudget;
-        c.status = kDone;
-    } else {
-        if (f < nf && c.t * c.T >= tf[f]) ev |= kEvFault;
-        if (c.save_nc >= 0.0 && c.t >= c.next_nc) ev |= kEvSnapshot;
-        if (c.save_ts >= 0.0 && c.t >= c.next_ts) ev |= kEvSeries;
-        if (ev) {
-            c.events = ev;
-            c.status = kPaused;
-        }
-    }
-    cp->t = c.t;
-    cp->dt = c.dt;
-    cp->step = c.step;
-    cp->parity = c.parity;
-    cp->jumping = c.jumping;
-    cp->dt_bits = c.dt_bits;
-    cp->tiles_done = c.tiles_done;
-    cp->events = c.events;
-    cp->status = c.status;
 }
 
 // Edge between rows gy-1 (a) and gy (b) of this lane's column, stencil rows
@@ -581,7 +515,7 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
     const int n = 2 * *nwork_ptr;
     // the deep kernels that read these lists claim units from zero (the
     // previous ones are done: this kernel runs after phase 1)
-    if (blockIdx.x == 0 && threadIdx.x < 2) claims[threadIdx.x] = 0;
+    if (blockIdx.x == 0 && threadIdx.x < 4) claims[threadIdx.x] = 0;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     __shared__ int cnt[2][kClassifyWarps];   // per warp: deep and general units of this round
     __shared__ int base2[2];                 // the block's first deep and general list slots
@@ -1507,17 +1441,6 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
     }
 }
 
-// Step controller of every running scenario, after both phase-2 kernels.
-__global__ void controller_kernel(const ScenarioDev *__restrict__ scen, int nslots)
-{
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nslots) return;
-    const ScenarioDev &s = scen[i];
-    if (!s.ctl || s.ctl->status != kRunning) return;
-    controller(s);
-}
-
-
 // One launch of deep phase PHASE / the general kernel in variant V.
 template <int PHASE, int V>
 static void launch_deep(const StepLaunch &L, cudaStream_t st)
@@ -1557,7 +1480,7 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
         break;
     case 3: launch_deep_any<2>(L, st); break;
     case 4: launch_general<2>(L, st); break;
-    default: controller_kernel<<<(L.nslots + 127) / 128, 128, 0, st>>>(L.scen, L.nslots); break;
+    default: launch_controller(L, st); break;
     }
 }
 

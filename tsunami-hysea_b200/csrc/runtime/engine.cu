@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <map>
@@ -141,7 +142,7 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
     b += 2 * (size_t)((nx + 2 * kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(UnitSum) + 1);
     b += kNumMaps * sizeof(TmaMap) + (size_t)(ny + 1) * sizeof(float4);
     if (has_faults) b += (size_t)nx * ny * sizeof(double);
-    return b + 4096;
+    return b + 4096 + kGaugeRing * sizeof(double);   // (gauges: 4 + 16 kGaugeRing + 8 bytes per point, not counted)
 }
 
 // ---------------------------------------------------------------------------
@@ -159,6 +160,9 @@ DevScenario::~DevScenario()
     if (maxbits) cudaFreeAsync(maxbits, ast);
     if (d_cells) cudaFreeAsync(d_cells, ast);
     if (d_gauge) cudaFreeAsync(d_gauge, ast);
+    if (d_gring) cudaFreeAsync(d_gring, ast);
+    if (d_gring_t) cudaFreeAsync(d_gring_t, ast);
+    if (d_gminmax) cudaFreeAsync(d_gminmax, ast);
     if (d_out) cudaFreeAsync(d_out, ast);
     if (fault_times_d) cudaFreeAsync(fault_times_d, ast);
     if (usum) cudaFreeAsync(usum, ast);
@@ -213,14 +217,21 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
         THY_CK(cudaStreamSynchronize(st));
     }
     if (!cells.empty()) {
-        THY_CK(cudaMallocAsync(&d_cells, cells.size() * sizeof(int), st));
-        THY_CK(cudaMallocAsync(&d_gauge, 4 * cells.size() * sizeof(float), st));
-        THY_CK(cudaMemcpyAsync(d_cells, cells.data(), cells.size() * sizeof(int), cudaMemcpyHostToDevice, st));
-        ts_min.assign(cells.size(), 1e30f);
-        ts_max.assign(cells.size(), -1e30f);
-        for (size_t i = 0; i < cells.size(); i++)
-            if (cells[i] < 0) ts_min[i] = ts_max[i] = -9999.0f;
+        // gauge cells, the ring of device samples and the extremes of eta
+        // (1e30 / -1e30 before the first sample; -9999 outside the grid)
+        const size_t np = cells.size();
+        THY_CK(cudaMallocAsync(&d_cells, np * sizeof(int), st));
+        THY_CK(cudaMallocAsync(&d_gauge, 4 * np * sizeof(float), st));
+        THY_CK(cudaMallocAsync(&d_gring, (size_t)kGaugeRing * 4 * np * sizeof(float), st));
+        THY_CK(cudaMallocAsync(&d_gring_t, kGaugeRing * sizeof(double), st));
+        THY_CK(cudaMallocAsync(&d_gminmax, np * sizeof(float2), st));
+        THY_CK(cudaMemcpyAsync(d_cells, cells.data(), np * sizeof(int), cudaMemcpyHostToDevice, st));
+        std::vector<float2> mm(np);
+        for (size_t i = 0; i < np; i++) mm[i] = cells[i] < 0 ? make_float2(-9999.0f, -9999.0f) : make_float2(1e30f, -1e30f);
+        THY_CK(cudaMemcpyAsync(d_gminmax, mm.data(), np * sizeof(float2), cudaMemcpyHostToDevice, st));
+        THY_CK(cudaStreamSynchronize(st));
     }
+    gauges_read = 0;
 
     // per-row metric terms: computed in FP64, stored once as FP32
     {
@@ -282,6 +293,13 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.vmax = (float)p->vmax;
     desc.dif_at = (float)p->dif_at;
     desc.sea = 0.f;
+    desc.gauge_cells = d_cells;
+    desc.ngauges = (int)cells.size();
+    desc.gauge_ring = d_gring;
+    desc.gauge_ring_t = d_gring_t;
+    desc.gauge_minmax = d_gminmax;
+    desc.Hs = Hs;
+    desc.Qs = Qs;
     for (int k = 0; k < 2; k++) {
         desc.eta[k] = fields + (0 + k) * plane;
         desc.qx[k] = fields + (2 + k) * plane;
@@ -529,8 +547,17 @@ public:
         THY_CK(cudaStreamWaitEvent(copy_st_, snap_ready_[k], 0));
         THY_CK(cudaMemcpyAsync(h_snap_ + k * 3 * n_, d, 3 * n_ * sizeof(float), cudaMemcpyDeviceToHost, copy_st_));
         THY_CK(cudaEventRecord(snap_copied_[k], copy_st_));
-        push(Job{0, index, time_s, k});
+        push(Job{0, index, time_s, k, {}});
         return THY_OK;
+    }
+
+    // Queues the delivery of a gauge sample the device already took (4
+    // floats per gauge, copied here).
+    void gauges_taken(int index, double time_s, const float *g4)
+    {
+        Job j{2, index, time_s, -1};
+        j.data.assign(g4, g4 + 4 * (size_t)np_);
+        push(j);
     }
 
     // Samples the gauges of the current state into a free slot and queues its delivery.
@@ -538,14 +565,14 @@ public:
     {
         const int k = acquire(ts_busy_, kTsSlots);
         float *d = d_ts_ + k * 4 * (size_t)np_;
-        launch_gauges(&s_->desc, s_->hctl.parity, s_->d_cells, np_, d, s_->Hs, s_->Qs, s_->Hmin, st);
+        launch_gauges(&s_->desc, s_->hctl.parity, s_->d_cells, np_, d, true, st);
         THY_CK(cudaGetLastError());
         THY_CK(cudaEventRecord(ts_ready_[k], st));
         THY_CK(cudaStreamWaitEvent(copy_st_, ts_ready_[k], 0));
         THY_CK(cudaMemcpyAsync(h_ts_ + k * 4 * (size_t)np_, d, 4 * (size_t)np_ * sizeof(float),
                                cudaMemcpyDeviceToHost, copy_st_));
         THY_CK(cudaEventRecord(ts_copied_[k], copy_st_));
-        push(Job{1, index, time_s, k});
+        push(Job{1, index, time_s, k, {}});
         return THY_OK;
     }
 
@@ -559,10 +586,11 @@ public:
 
 private:
     struct Job {
-        int kind;     // 0 snapshot, 1 gauges
+        int kind;     // 0 snapshot, 1 gauges in a slot, 2 gauges in `data`
         int index;
         double time;
         int slot;
+        std::vector<float> data;
     };
 
     int acquire(bool *busy, int n)
@@ -578,11 +606,11 @@ private:
         }
     }
 
-    void push(const Job &j)
+    void push(Job j)
     {
         {
             std::lock_guard<std::mutex> lk(m_);
-            q_.push_back(j);
+            q_.push_back(std::move(j));
         }
         cv_.notify_all();
     }
@@ -595,14 +623,14 @@ private:
                 std::unique_lock<std::mutex> lk(m_);
                 cv_.wait(lk, [this] { return stop_ || !q_.empty(); });
                 if (q_.empty()) return;
-                j = q_.front();
+                j = std::move(q_.front());
                 q_.pop_front();
                 busy_ = true;
             }
             deliver(j);
             {
                 std::lock_guard<std::mutex> lk(m_);
-                (j.kind == 0 ? snap_busy_ : ts_busy_)[j.slot] = false;
+                if (j.kind < 2) (j.kind == 0 ? snap_busy_ : ts_busy_)[j.slot] = false;
                 busy_ = false;
             }
             cv_.notify_all();
@@ -620,20 +648,22 @@ private:
             o_->on_snapshot(o_->user, j.index, j.time, h, h + n_, h + 2 * n_);
             return;
         }
-        if (cudaEventSynchronize(ts_copied_[j.slot]) != cudaSuccess) {
-            set_error();
-            return;
+        const float *g;
+        if (j.kind == 1) {
+            if (cudaEventSynchronize(ts_copied_[j.slot]) != cudaSuccess) {
+                set_error();
+                return;
+            }
+            g = h_ts_ + j.slot * 4 * (size_t)np_;
+        } else {
+            g = j.data.data();
         }
-        const float *g = h_ts_ + j.slot * 4 * (size_t)np_;
+        // (the extremes of eta are folded on the device with every sample)
         std::vector<float> e(np_), ux(np_), uy(np_);
         for (int i = 0; i < np_; i++) {
             e[i] = g[4 * i];
             ux[i] = g[4 * i + 1];
             uy[i] = g[4 * i + 2];
-            if (s_->cells[i] >= 0) {
-                s_->ts_min[i] = (s_->ts_min[i] < e[i]) ? s_->ts_min[i] : e[i];
-                s_->ts_max[i] = (e[i] < s_->ts_max[i]) ? s_->ts_max[i] : e[i];
-            }
         }
         if (o_ && o_->on_series) o_->on_series(o_->user, j.index, j.time, e.data(), ux.data(), uy.data());
     }
@@ -692,6 +722,31 @@ int DevScenario::sample_gauges(const thy_outputs *o, cudaStream_t st)
     return THY_OK;
 }
 
+// Gauge samples the step controller took since the last call (at most
+// kGaugeRing: the host reads them after every chunk), handed to the output
+// pipe in time order, before any event the host performs at the chunk's end.
+int DevScenario::read_device_gauges(const thy_outputs *o, cudaStream_t st)
+{
+    const unsigned n = hctl.gauge_count - gauges_read;
+    if (n == 0 || cells.empty()) return THY_OK;
+    if (n > (unsigned)kGaugeRing) return THY_ERR_INVALID;   // more samples than the ring holds: not read in time
+    const size_t np = cells.size();
+    std::vector<float> ring((size_t)kGaugeRing * 4 * np);
+    double ring_t[kGaugeRing];
+    THY_CK(cudaMemcpyAsync(ring.data(), d_gring, ring.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+    THY_CK(cudaMemcpyAsync(ring_t, d_gring_t, sizeof(ring_t), cudaMemcpyDeviceToHost, st));
+    THY_CK(cudaStreamSynchronize(st));
+    int rc;
+    if ((rc = open_outputs(o, st))) return rc;
+    for (unsigned k = gauges_read; k != hctl.gauge_count; k++) {
+        const unsigned slot = k % kGaugeRing;
+        if (pipe) pipe->gauges_taken(series, ring_t[slot], ring.data() + (size_t)slot * 4 * np);
+        series++;
+    }
+    gauges_read = hctl.gauge_count;
+    return THY_OK;
+}
+
 int DevScenario::finish(const thy_outputs *o, cudaStream_t st)
 {
     int rc;
@@ -707,13 +762,16 @@ int DevScenario::finish(const thy_outputs *o, cudaStream_t st)
     const int np = (int)cells.size();
     if (np > 0 && (o->series_min || o->series_max || o->series_bathy)) {
         std::vector<float> g(4 * (size_t)np);
-        launch_gauges(&desc, hctl.parity, d_cells, np, d_gauge, Hs, Qs, Hmin, st);
+        std::vector<float2> mm(np);
+        // the depths of the final state (not a sample: no fold) and the extremes
+        launch_gauges(&desc, hctl.parity, d_cells, np, d_gauge, false, st);
         THY_CK(cudaGetLastError());
         THY_CK(cudaMemcpyAsync(g.data(), d_gauge, g.size() * sizeof(float), cudaMemcpyDeviceToHost, st));
+        THY_CK(cudaMemcpyAsync(mm.data(), d_gminmax, np * sizeof(float2), cudaMemcpyDeviceToHost, st));
         THY_CK(cudaStreamSynchronize(st));
         for (int i = 0; i < np; i++) {
-            if (o->series_min) o->series_min[i] = ts_min[i];
-            if (o->series_max) o->series_max[i] = ts_max[i];
+            if (o->series_min) o->series_min[i] = mm[i].x;
+            if (o->series_max) o->series_max[i] = mm[i].y;
             if (o->series_bathy) o->series_bathy[i] = g[4 * i + 3];
         }
     }
@@ -741,6 +799,109 @@ Batch::~Batch()
     if (ev_fork) cudaEventDestroy(ev_fork);
     if (ev_join) cudaEventDestroy(ev_join);
     if (st_side) cudaStreamDestroy(st_side);
+    if (owns_stream && st) cudaStreamDestroy(st);
+}
+
+void Batch::reset_counters()
+{
+    device_ms = 0;
+    launches = 0;
+    chunks_run = 0;
+    captures = 0;
+    capture_s = 0;
+    tune_samples = 0;
+}
+
+namespace {
+struct RunPool {
+    std::mutex mu;
+    std::vector<std::pair<Batch *, bool>> batches;   // (batch, leased)
+};
+// never destroyed: batches still held at process exit are left to the driver
+RunPool &run_pool()
+{
+    static RunPool *p = new RunPool();
+    return *p;
+}
+constexpr size_t kRunPoolMax = 8;   // idle batches kept per process
+}  // namespace
+
+Batch *lease_run_batch(int device, int max_work, int *rc)
+{
+    *rc = THY_OK;
+    RunPool &P = run_pool();
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        // the smallest idle batch of this device that holds the work, within
+        // 16x of it (grids follow the capacity)
+        int best = -1;
+        for (int i = 0; i < (int)P.batches.size(); i++) {
+            Batch *b = P.batches[i].first;
+            if (P.batches[i].second || b->device != device || b->work_capacity < max_work ||
+                b->work_capacity > 16 * std::max(max_work, 64))
+                continue;
+            if (best < 0 || b->work_capacity < P.batches[best].first->work_capacity) best = i;
+        }
+        if (best >= 0) {
+            P.batches[best].second = true;
+            Batch *b = P.batches[best].first;
+            b->reset_counters();
+            return b;
+        }
+    }
+    Batch *b = new Batch();
+    cudaStream_t st = nullptr;
+    if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+        cudaGetLastError();
+        delete b;
+        *rc = THY_ERR_CUDA;
+        return nullptr;
+    }
+    b->owns_stream = true;
+    if ((*rc = b->init(1, max_work, st))) {
+        b->st = st;
+        delete b;
+        return nullptr;
+    }
+    std::lock_guard<std::mutex> g(P.mu);
+    P.batches.emplace_back(b, true);
+    return b;
+}
+
+void return_run_batch(Batch *b, bool healthy)
+{
+    if (!b) return;
+    RunPool &P = run_pool();
+    Batch *drop = nullptr;
+    {
+        std::lock_guard<std::mutex> g(P.mu);
+        for (size_t i = 0; i < P.batches.size(); i++)
+            if (P.batches[i].first == b) {
+                if (!healthy) {
+                    P.batches.erase(P.batches.begin() + i);
+                    drop = b;
+                } else {
+                    P.batches[i].second = false;
+                }
+                break;
+            }
+        if (!drop) {
+            // keep at most kRunPoolMax idle batches: drop the oldest idle one
+            size_t idle = 0;
+            for (auto &e : P.batches) idle += e.second ? 0 : 1;
+            if (idle > kRunPoolMax)
+                for (size_t i = 0; i < P.batches.size(); i++)
+                    if (!P.batches[i].second) {
+                        drop = P.batches[i].first;
+                        P.batches.erase(P.batches.begin() + i);
+                        break;
+                    }
+        }
+    }
+    if (drop) {
+        cudaStreamSynchronize(drop->st);
+        delete drop;
+    }
 }
 
 int Batch::init(int cap, int max_work, cudaStream_t stream)
@@ -758,8 +919,8 @@ int Batch::init(int cap, int max_work, cudaStream_t stream)
     THY_CK(cudaMallocAsync(&d_nwork0, sizeof(int), st));
     THY_CK(cudaMallocAsync(&d_lists, (2 + 4 * (size_t)std::max(max_work, 1)) * sizeof(int), st));
     THY_CK(cudaMemsetAsync(d_lists, 0, 2 * sizeof(int), st));
-    THY_CK(cudaMallocAsync(&d_claims, 2 * sizeof(int), st));
-    THY_CK(cudaMemsetAsync(d_claims, 0, 2 * sizeof(int), st));
+    THY_CK(cudaMallocAsync(&d_claims, 4 * sizeof(int), st));
+    THY_CK(cudaMemsetAsync(d_claims, 0, 4 * sizeof(int), st));
     THY_CK(cudaEventCreate(&ev0));
     THY_CK(cudaEventCreate(&ev1));
     THY_CK(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
@@ -900,7 +1061,7 @@ long long Batch::steps_to_event(const DevScenario &s)
     const ScenarioCtl &c = s.hctl;
     double horizon = c.t_end;
     if (c.save_nc >= 0.0) horizon = std::min(horizon, c.next_nc);
-    if (c.save_ts >= 0.0) horizon = std::min(horizon, c.next_ts);
+    // (gauge times do not: the controller samples the gauges on the device)
     const int nf = (int)(s.faults.size() / 10);
     if (c.fault_next < nf) horizon = std::min(horizon, s.faults[10 * c.fault_next] / s.Ts);
     long long n = (c.dt > 0.0) ? (long long)std::ceil((horizon - c.t) / c.dt) : 1;
@@ -908,13 +1069,7 @@ long long Batch::steps_to_event(const DevScenario &s)
     return std::max(1ll, n);
 }
 
-int Batch::chunk_for(long long steps) const
-{
-    if (steps >= chunk) return chunk;
-    int len = 1;
-    while (2 * len <= steps) len *= 2;
-    return len;
-}
+int Batch::chunk_for(long long steps) const { return (int)std::max(1ll, std::min<long long>(steps, chunk)); }
 
 int Batch::rebuild()
 {
@@ -938,10 +1093,11 @@ StepLaunch Batch::params() const
     L.claims = d_claims;
     L.cap = 2 * work_capacity;   // lists hold work units (two per work-list entry)
     L.tiling = tiling;
-    // general kernel: a grid of 8 waves of resident CTAs striding over the
-    // list; deep kernels: persistent, one wave
+    // general kernel: one CTA per SM more than are resident, striding over
+    // the list (measured at 4096^2 against 8 waves: 0.2965 against 0.3024 ms
+    // a step); deep kernels: persistent, one wave
     const int sms = device_sm_count();
-    L.grid = std::max(1, std::min(2 * work_capacity, sms * std::max(1, step_blocks_per_sm(tiling.general)) * 8));
+    L.grid = std::max(1, std::min(2 * work_capacity, sms * (std::max(1, step_blocks_per_sm(tiling.general)) + 1)));
     L.deep_grid[0] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(1, tiling.deep1))));
     L.deep_grid[1] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(2, tiling.deep2))));
     L.classify_grid = std::max(1, std::min((2 * work_capacity + 255) / 256, 4 * device_sm_count()));
@@ -977,15 +1133,19 @@ int Batch::run_chunk(bool timed, int len)
     if (len <= 0 || len > chunk) len = chunk;
     const TuneKey key = tune_key(&known);
     if ((rc = use_tiling(tuner_pick(key, &sampling)))) return rc;
+    // a full chunk is one graph launch; a shorter one launches the 1-step
+    // graph `len` times (two captures per tiling in all)
     cudaGraphExec_t exec = gexec;
+    int repeat = 1;
     if (len != chunk) {
         exec = nullptr;
         for (auto &g : graphs)
-            if (g.tiling == tiling && g.len == len) exec = g.exec;
+            if (g.tiling == tiling && g.len == 1) exec = g.exec;
         if (!exec) {
-            if ((rc = capture(len))) return rc;
+            if ((rc = capture(1))) return rc;
             exec = graphs.back().exec;
         }
+        repeat = len;
     }
     // a sample needs a chunk in which every running member steps `chunk`
     // times (no member reaches its end or an event before the chunk's last
@@ -1002,7 +1162,7 @@ int Batch::run_chunk(bool timed, int len)
             running++;
         }
     if (timed) THY_CK(cudaEventRecord(ev0, st));
-    THY_CK(cudaGraphLaunch(exec, st));
+    for (int i = 0; i < repeat; i++) THY_CK(cudaGraphLaunch(exec, st));
     if (timed) THY_CK(cudaEventRecord(ev1, st));
     THY_CK(cudaMemcpyAsync(h_ctl, d_ctl, capacity * sizeof(ScenarioCtl), cudaMemcpyDeviceToHost, st));
     THY_CK(cudaStreamSynchronize(st));
@@ -1198,16 +1358,18 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
     if (rc) return rc;
     if (!p) return THY_ERR_INVALID;
     const auto t_start = std::chrono::steady_clock::now();
-    cudaStream_t st;
-    THY_CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if (stats) std::memset(stats, 0, sizeof(*stats));
+    int device = 0;
+    THY_CK(cudaGetDevice(&device));
+    Batch *bp = lease_run_batch(device, (p->nx / kTileX + 2) * (p->ny / kTileY + 2), &rc);
+    if (!bp) return rc;
+    Batch &b = *bp;
+    cudaStream_t st = b.st;
     auto t0 = std::chrono::steady_clock::now();
     auto t_release = t0;
     double event_s = 0;
-    if (stats) std::memset(stats, 0, sizeof(*stats));
     {
         DevScenario s;
-        Batch b;
-        if ((rc = b.init(1, (p->nx / kTileX + 2) * (p->ny / kTileY + 2), st))) goto out;
         if ((rc = b.attach(&s))) goto out;
         if ((rc = s.setup(p, st))) goto out;
         s.desc.ctl = s.ctl;
@@ -1235,6 +1397,7 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
             // scenario paused
             do {
                 if ((rc = b.run_chunk(true, b.chunk_for(Batch::steps_to_event(s))))) goto out;
+                if ((rc = s.read_device_gauges(o, st))) goto out;
             } while (s.hctl.status == kRunning);
             if (s.hctl.status == kFailed) { rc = failure_code(s.hctl); goto out; }
         }
@@ -1268,8 +1431,15 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
         }
     out:
         t_release = std::chrono::steady_clock::now();
+        b.detach(&s);
     }
-    cudaStreamDestroy(st);
+    {
+        // the batch goes back to the pool unless the run ended in a CUDA
+        // error (its state is then unknown); its stream is idle
+        const bool healthy = cudaStreamSynchronize(st) == cudaSuccess && rc != THY_ERR_CUDA && rc != THY_ERR_TIMEOUT;
+        if (!healthy) cudaGetLastError();
+        return_run_batch(bp, healthy);
+    }
     if (stats) {
         const auto t_end = std::chrono::steady_clock::now();
         stats->release_seconds = std::chrono::duration<double>(t_end - t_release).count();

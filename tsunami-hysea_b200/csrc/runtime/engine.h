@@ -46,6 +46,10 @@ struct DevScenario {
     unsigned int *maxbits = nullptr;
     int *d_cells = nullptr;        // gauge cells
     float *d_gauge = nullptr;      // 4 floats per gauge
+    float *d_gring = nullptr;      // kGaugeRing device samples x 4 floats per gauge (desc.gauge_ring)
+    double *d_gring_t = nullptr;   // their times (desc.gauge_ring_t)
+    float2 *d_gminmax = nullptr;   // per gauge extremes of eta (desc.gauge_minmax)
+    unsigned gauges_read = 0;      // device samples handed to the outputs so far
     float *d_out = nullptr;        // 3 planes nx*ny for snapshots / outputs
     double *fault_times_d = nullptr;
     UnitSum *usum = nullptr;       // 2 parities x 2 ntiles unit depth summaries (desc.usum)
@@ -69,7 +73,6 @@ struct DevScenario {
     ScenarioCtl hctl{};
     // run bookkeeping
     int snapshots = 0, series = 0;
-    std::vector<float> ts_min, ts_max;
     double first_dt_s = 0;
     // work mix of the last chunk it stepped (per step): deep units, skipped
     // dry units; the autotuner's key for the chunks that follow
@@ -90,6 +93,7 @@ struct DevScenario {
     int open_outputs(const thy_outputs *o, cudaStream_t st);
     int snapshot(const thy_outputs *o, cudaStream_t st);
     int sample_gauges(const thy_outputs *o, cudaStream_t st);
+    int read_device_gauges(const thy_outputs *o, cudaStream_t st);   // the controller's samples since the last call
     int finish(const thy_outputs *o, cudaStream_t st);
 };
 
@@ -114,8 +118,8 @@ struct Batch {
     int device = 0;
     Tiling tiling;                     // of gexec
     // step graphs captured for the current capacity, per tiling and length:
-    // the full chunk, and the shorter power-of-two chunks that make a step
-    // count exact (a session's last steps, the steps before an event)
+    // the full chunk, and one step, launched as often as a shorter chunk
+    // needs (a session's last steps, the steps before an event)
     struct Graph {
         Tiling tiling;
         int len;
@@ -133,6 +137,8 @@ struct Batch {
     long long chunks_run = 0;          // graph launches
     long long captures = 0;            // graphs captured
     double capture_s = 0;              // host time spent capturing and instantiating them
+    bool owns_stream = false;          // st was created for the batch (pooled batches of thy_run)
+    void reset_counters();             // the per-run counters above, and the tuning samples
 
     ~Batch();
     int init(int capacity, int max_work, cudaStream_t stream);
@@ -148,16 +154,15 @@ struct Batch {
     void drop_graphs();
     int rebuild();                    // update(), and capture() when there is no graph yet
     int initial_dt_of(DevScenario *s);   // initial dt of one member (phase 0 over its units only)
-    // one graph launch of `len` steps (0 or more than `chunk`: the full
-    // chunk; otherwise a power of two below it) + control download
+    // `len` steps (0 or more than `chunk`: the full chunk, one graph launch;
+    // fewer: the 1-step graph launched len times) + control download
     // (synchronous); the tiling is the autotuner's pick, and a full timed
     // chunk is one of its samples
     int run_chunk(bool timed, int len = 0);
     // steps a member can take before its next event or its end, estimated
     // from its current dt (at least 1)
     static long long steps_to_event(const DevScenario &s);
-    // the longest graph (a power of two, at most `chunk`) that does not
-    // overshoot `steps`
+    // the chunk length for `steps` steps: at most `chunk`, at least 1
     int chunk_for(long long steps) const;
     // the autotuner's key of the next chunk: this device, the deep and
     // general units per step estimated from each stepping member's last
@@ -167,6 +172,13 @@ struct Batch {
     StepLaunch params() const;
     int reset_lists();               // classify again: after the host changed a member's state
 };
+
+// Single-scenario batches of thy_run, kept per device between runs with
+// their buffers, stream and captured graphs, so that a run of a grid size the
+// process has run before captures no graph.  A lease hands a batch with at
+// least `max_work` work items to one caller at a time.
+Batch *lease_run_batch(int device, int max_work, int *rc);
+void return_run_batch(Batch *b, bool healthy);   // healthy = false: destroy it instead
 
 int ensure_device();
 int device_sm_count();

@@ -300,11 +300,16 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             if (S->slots[i] && sel[i]) horizon = std::min(horizon, Batch::steps_to_event(*S->slots[i]->s));
         if ((rc = S->b.run_chunk(true, S->b.chunk_for(horizon)))) return rc;
         S->stats.chunks++;
-        // retire what finished in this chunk right away
+        // hand on the gauge samples the chunk took; retire what finished in
+        // this chunk right away
         for (int i = 0; i < cap; i++) {
             Active *a = S->slots[i];
             if (!a) continue;
-            const DevScenario &s = *a->s;
+            DevScenario &s = *a->s;
+            if ((rc = s.read_device_gauges(a->r.o, S->st))) {
+                complete(S, i, rc);
+                continue;
+            }
             if (s.hctl.status == kFailed) complete(S, i, failure_code(s.hctl));
             else if (!(s.hctl.t < s.t_end) || (s.max_steps >= 0 && s.hctl.step >= s.max_steps))
                 complete(S, i, THY_OK);

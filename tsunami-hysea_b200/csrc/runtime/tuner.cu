@@ -145,6 +145,28 @@ int tune_bucket(double units)
     return b;
 }
 
+// Steps of at most kSmallWork units (deep + general, from the buckets' upper
+// bounds) are not tuned: the kernels then have fewer units than the GPU has
+// resident CTAs, each runs at the latency of one unit, and the graph
+// captures a search costs would outweigh what it could find.  They run the
+// tiling with the shortest per-warp row chains in the phase-2 kernels (deep
+// phase 2 and the general kernel in their most row groups), which the search
+// picked at 512 x 512 (13.9 against 17.7 ms of device time for 259 steps
+// with the default tiling).
+constexpr long long kSmallWork = 512;
+bool small_work(const TuneKey &k)
+{
+    return k.deep < 40 && k.general < 40 && (1ll << k.deep) + (1ll << k.general) <= kSmallWork;
+}
+Tiling small_tiling()
+{
+    Tiling t;
+    t.deep1 = 0;
+    t.deep2 = 2;
+    t.general = 2;
+    return t;
+}
+
 Tiling tuner_pick(const TuneKey &k, bool *sampling)
 {
     State &s = state();
@@ -153,6 +175,7 @@ Tiling tuner_pick(const TuneKey &k, bool *sampling)
     *sampling = false;
     if (s.forced) return s.force;
     if (s.off) return Tiling();
+    if (small_work(k)) return small_tiling();
     if (e.done) return e.inc;
     *sampling = true;
     return candidate(e, e.pos % 3);
@@ -163,7 +186,7 @@ void tuner_sample(const TuneKey &k, const Tiling &t, double v)
     State &s = state();
     std::lock_guard<std::mutex> g(s.mu);
     Entry &e = entry(s, k);
-    if (s.forced || s.off || e.done) return;
+    if (s.forced || s.off || e.done || small_work(k)) return;
     const int j = e.pos % 3;
     if (t != candidate(e, j) || !(v > 0.0)) return;   // a stale tiling (another batch switched first)
     if (v < e.best[j]) e.best[j] = v;
@@ -191,6 +214,10 @@ bool tuner_decided(const TuneKey &k, Tiling *best)
     }
     if (s.off) {
         if (best) *best = Tiling();
+        return true;
+    }
+    if (small_work(k)) {
+        if (best) *best = small_tiling();
         return true;
     }
     if (best) *best = e.inc;

@@ -11,6 +11,10 @@
 // minimum of each kept; an alternative replaces the incumbent when it is more
 // than 1 % faster.  A decided key runs its best tiling from then on.
 //
+// Steps of at most 512 work units are not tuned: they run the tiling with
+// the most row groups in the phase-2 kernels (deep 1 default, deep 2 and
+// general variant 2).
+//
 // Environment: THY_TILING="d1,d2,g" forces a tiling (variant indices);
 // THY_TUNE=0 keeps the default tiling; THY_TUNE_CACHE=<file> keeps decided
 // keys across processes (one line per key: device name, SM count, deep and
