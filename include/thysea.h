@@ -271,9 +271,9 @@ typedef struct thy_server_opts {
     long long hbm_budget_bytes;   /* device memory for scenario state (0: 90 % of the free memory) */
     int max_scenarios;            /* scenarios resident at once (0: 256) */
     int device;
-    long long chunk_cells;        /* cells stepped per chunk: the resident scenarios with the least
-                                     remaining work (cells x remaining steps) are stepped until their
-                                     cells reach this, at least one (0: 32 M; < 0: all) */
+    long long chunk_cells;        /* cells stepped per chunk: the resident scenario submitted first,
+                                     then those with the least remaining work (cells x remaining
+                                     steps), until their cells reach this (0: 32 M; < 0: all) */
 } thy_server_opts;
 typedef struct thy_server_stats {
     long long submitted, admitted, completed, failed, cancelled, rejected;

@@ -182,3 +182,24 @@ def test_gauges_sampled_on_the_device_do_not_stop_the_run(gpu):
     nu = len(r["series"]["min"])
     assert np.abs(g["series"]["min"][:nu] - r["series"]["min"]).max() <= ETA_TOL_M
     assert np.abs(g["series"]["max"][:nu] - r["series"]["max"]).max() <= ETA_TOL_M
+
+
+@pytest.mark.parametrize("lat_centre", [70.0, -80.0])
+def test_high_latitude_metric_terms(gpu, lat_centre):
+    """far from the equator (cos(lat) 0.34 at 70 degrees, 0.17 at 80): the
+    spherical metric terms (cos(lat), dlat / cos(lat), the cell area, dlon)
+    are formed in FP64 on the host once and kept in FP32 row tables; the
+    surface, the maximum height and the gauges stay within the tolerances of
+    the FP64 oracle, which keeps them in FP64 throughout"""
+    p = synth.plain_small(nx=256, ny=224, sim_time=600.0, save_time=200.0, series_time=60.0, npoints=8)
+    p.name = f"lat{int(lat_centre)}"
+    p.lat = p.lat + lat_centre
+    p.faults[0].lat += lat_centre
+    p.points = p.points.copy()
+    p.points[:, 1] += lat_centre
+    g, r, c = _both(gpu, p)
+    _assert_parity(c)
+    assert g["nseries"] == r["nseries"]
+    assert np.abs(np.asarray(g["series"]["eta"]) - r["series"]["eta"]).max() <= ETA_TOL_M
+    # the wave is there: the fault deformed the surface by more than the tolerance
+    assert float(np.abs(r["max_height"][r["max_height"] != -9999.0]).max()) > 100 * ETA_TOL_M

@@ -393,12 +393,28 @@ __device__ __forceinline__ unsigned long long global_ns()
 // context that is time-sliced or pre-empted on a shared GPU does not take a
 // healthy copy for a lost one.
 constexpr unsigned long long kWaitNs = 4000000000ull;
+// try_wait that may suspend the thread for up to hint_ns while the phase is
+// incomplete (it resumes as soon as the phase completes), so that waiting
+// warps do not take issue slots from the warps that compute
+__device__ __forceinline__ bool mbar_try_wait_hint(uint64_t *bar, uint32_t parity, uint32_t hint_ns)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity), "r"(hint_ns)
+        : "memory");
+    return ok != 0;
+}
+constexpr uint32_t kSuspendNs = 1000000;   // at most 1 ms per try
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity)
 {
     if (mbar_try_wait(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (int i = 0; i < (1 << 28); i++) {
-        if (mbar_try_wait(bar, parity)) return true;
+        if (mbar_try_wait_hint(bar, parity, kSuspendNs)) return true;
         if (global_ns() - t0 > kWaitNs) return false;
     }
     return false;

@@ -257,14 +257,23 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
     // arithmetic changes.
     std::vector<char> sel(cap, 0);
     if (any_running) {
+        // the request submitted first is always stepped (so that no request
+        // waits behind a stream of smaller ones: the tail of time-to-result),
+        // the others by least remaining work
         std::vector<std::pair<double, int>> order;
+        int first = -1;
+        for (int i = 0; i < cap; i++) {
+            Active *a = S->slots[i];
+            if (!a) continue;
+            if (first < 0 || a->r.submitted < S->slots[first]->r.submitted) first = i;
+        }
         for (int i = 0; i < cap; i++) {
             Active *a = S->slots[i];
             if (!a) continue;
             const DevScenario &s = *a->s;
             const double cells = (double)s.nx * s.ny;
             const double steps = s.hctl.dt > 0.0 ? (s.t_end - s.hctl.t) / s.hctl.dt : 0.0;
-            order.emplace_back(cells * std::max(steps, 1.0), i);
+            order.emplace_back(i == first ? -1.0 : cells * std::max(steps, 1.0), i);
         }
         std::sort(order.begin(), order.end());
         double taken = 0.0;
