@@ -273,7 +273,8 @@ typedef struct thy_server_opts {
     int device;
     long long chunk_cells;        /* cells stepped per chunk: the resident scenario submitted first,
                                      then those with the least remaining work (cells x remaining
-                                     steps), until their cells reach this (0: 32 M; < 0: all) */
+                                     steps), until their cells reach this (0: 2^24, one 4096^2 grid;
+                                     < 0: all) */
 } thy_server_opts;
 typedef struct thy_server_stats {
     long long submitted, admitted, completed, failed, cancelled, rejected;

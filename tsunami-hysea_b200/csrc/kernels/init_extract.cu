@@ -215,6 +215,16 @@ __global__ void __launch_bounds__(kControllerThreads) controller_kernel(const Sc
     (void)nslots;
 }
 
+cudaError_t preload_output_kernels()
+{
+    cudaFuncAttributes a;
+    cudaError_t e;
+    if ((e = cudaFuncGetAttributes(&a, controller_kernel)) || (e = cudaFuncGetAttributes(&a, init_state_kernel)) ||
+        (e = cudaFuncGetAttributes(&a, extract_kernel)) || (e = cudaFuncGetAttributes(&a, gauges_kernel)))
+        return e;
+    return cudaSuccess;
+}
+
 void launch_controller(const StepLaunch &L, cudaStream_t st)
 {
     controller_kernel<<<L.nslots, kControllerThreads, 0, st>>>(L.scen, L.nslots);

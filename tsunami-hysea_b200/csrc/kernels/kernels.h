@@ -97,6 +97,9 @@ void launch_initial_dt(const StepLaunch &L, cudaStream_t st);
 void launch_lists_current(const StepLaunch &L, cudaStream_t st);
 // init_extract.cu: the step controller of every slot (launch 5 of a step)
 void launch_controller(const StepLaunch &L, cudaStream_t st);
+// init_extract.cu / okada.cu: load their kernels now rather than at first use
+cudaError_t preload_output_kernels();
+cudaError_t preload_okada_kernels();
 int deep_blocks_per_sm(int phase, int variant);
 
 // init.cu: double-precision host state (reference layout, dimensionless) to

@@ -175,4 +175,14 @@ void launch_apply_deformation(const ScenarioDev *s_host, const double *def, int 
     apply_deformation_kernel<<<grid, 256, 0, st>>>(*s_host, def, crop_flag, crop_value, max_bits);
 }
 
+cudaError_t preload_okada_kernels()
+{
+    cudaFuncAttributes a;
+    cudaError_t e;
+    if ((e = cudaFuncGetAttributes(&a, okada_kernel)) || (e = cudaFuncGetAttributes(&a, absmax_kernel)) ||
+        (e = cudaFuncGetAttributes(&a, apply_deformation_kernel)))
+        return e;
+    return cudaSuccess;
+}
+
 }  // namespace thy

@@ -522,7 +522,7 @@ __device__ __forceinline__ const int *general_items(const int *lists, int cap) {
 // changed has unknown (NaN) summaries, so its units are general.  Units below
 // the grid (the lower half of a last tile row of <= 16 rows) are not listed.
 // The counts are zeroed before the launch.
-constexpr int kClassifyThreads = 256, kClassifyWarps = kClassifyThreads / 32;
+constexpr int kClassifyThreads = 128, kClassifyWarps = kClassifyThreads / 32;
 __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const ScenarioDev *__restrict__ scen,
                                                                    const int2 *__restrict__ work,
                                 const int *__restrict__ nwork_ptr, int *__restrict__ lists, int cap, int before_step,
@@ -538,6 +538,7 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int u = base + threadIdx.x;
         bool listed = false, deep = false;
+        ScenarioCtl *dry_ctl = nullptr;   // the scenario of a unit skipped as dry land this step
         if (u < n) {
             const int2 item = work[u >> 1];
             const ScenarioDev &s = scen[item.x];
@@ -558,9 +559,15 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
                 }
                 if (age >= kDryAge) {
                     listed = false;
-                    if (running) atomicAdd(&ctl->units_dry, 1ull);
+                    if (running) dry_ctl = ctl;
                 }
             }
+        }
+        // dry units counted with one atomic per scenario and warp (the lanes
+        // of a warp can belong to different scenarios of a batch)
+        {
+            const unsigned peers = __match_any_sync(0xffffffffu, (unsigned long long)dry_ctl);
+            if (dry_ctl && lane == __ffs(peers) - 1) atomicAdd(&dry_ctl->units_dry, (unsigned long long)__popc(peers));
         }
         // block-aggregated appends: one atomic per list and block (the
         // counters are two words that every block appends to)
@@ -1522,9 +1529,23 @@ static cudaError_t configure_deep()
     return cudaFuncSetAttribute(f, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
 }
 
+// Loads every step kernel now (module loading is otherwise lazy, at a
+// kernel's first launch or graph instantiation: inside the first run's loop).
+template <typename F>
+static cudaError_t preload(F *f)
+{
+    cudaFuncAttributes a;
+    return cudaFuncGetAttributes(&a, f);
+}
+
 cudaError_t configure_step_kernels()
 {
     cudaError_t e;
+    if ((e = preload(step_kernel<0, general_ng(0)>)) || (e = preload(step_kernel<1, general_ng(0)>)) ||
+        (e = preload(step_kernel<1, general_ng(1)>)) || (e = preload(step_kernel<1, general_ng(2)>)) ||
+        (e = preload(step_kernel<2, general_ng(0)>)) || (e = preload(step_kernel<2, general_ng(1)>)) ||
+        (e = preload(step_kernel<2, general_ng(2)>)) || (e = preload(classify_kernel)))
+        return e;
     if ((e = configure_deep<1, 0>()) || (e = configure_deep<1, 1>()) || (e = configure_deep<1, 2>()) ||
         (e = configure_deep<2, 0>()) || (e = configure_deep<2, 1>()) || (e = configure_deep<2, 2>()))
         return e;

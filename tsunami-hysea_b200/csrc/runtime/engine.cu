@@ -55,6 +55,8 @@ int ensure_device()
     THY_CK(cudaSetDevice(g_device));
     if (!g_configured[g_device]) {
         THY_CK(configure_step_kernels());
+        THY_CK(preload_output_kernels());
+        THY_CK(preload_okada_kernels());
         // device buffers come from the stream-ordered default pool; freed
         // memory stays in the pool for the next scenario instead of going
         // back to the driver
@@ -1100,7 +1102,7 @@ StepLaunch Batch::params() const
     L.grid = std::max(1, std::min(2 * work_capacity, sms * (std::max(1, step_blocks_per_sm(tiling.general)) + 1)));
     L.deep_grid[0] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(1, tiling.deep1))));
     L.deep_grid[1] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(2, tiling.deep2))));
-    L.classify_grid = std::max(1, std::min((2 * work_capacity + 255) / 256, 4 * device_sm_count()));
+    L.classify_grid = std::max(1, std::min((2 * work_capacity + 127) / 128, 8 * device_sm_count()));
     L.nslots = capacity;
     return L;
 }

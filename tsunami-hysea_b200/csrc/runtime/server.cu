@@ -148,7 +148,9 @@ extern "C" int thy_server_open(const thy_server_opts *opts, thy_server **out)
     THY_CK(cudaMemGetInfo(&free_b, &total_b));
     thy_server *S = new thy_server();
     S->budget = o.hbm_budget_bytes ? (size_t)o.hbm_budget_bytes : free_b / 10 * 9;
-    S->chunk_cells = o.chunk_cells ? o.chunk_cells : 32ll << 20;
+    // by default one 4096^2 grid's cells: enough work to fill the GPU, and a
+    // large request runs alone at its own speed instead of sharing its steps
+    S->chunk_cells = o.chunk_cells ? o.chunk_cells : 1ll << 24;
     const int cap = o.max_scenarios > 0 ? o.max_scenarios : 256;
     // work-list capacity: the tiles of the budget's worth of cells, at least one grid of 4096^2
     const size_t cells = S->budget / 40 + (size_t)4096 * 4096;
