@@ -122,6 +122,12 @@ struct ScenarioDev {
     // per unit: consecutive classifications that found its 3 x 3 unit
     // neighbourhood dry (saturating)
     unsigned char *dry_age;
+    // per unit: the largest |dep1 - dep0| between the two cells of an edge of
+    // the unit's cells (x edges x0 .. x0+112 of its rows, y edges yb .. yb+16
+    // of its columns, inside the grid); fixed between faults.  A deep unit
+    // whose unit and two-cell ring are all deeper than this steps its
+    // surface jumps as the plain difference (see surface_jump)
+    float *unit_gmax;
     // TMA tensor maps of the field planes (kMap* order), null when the grid
     // is too small to have deep tiles
     const struct TmaMap *tmap;
@@ -226,7 +232,9 @@ __device__ __forceinline__ float blend_2s(float hij, float hpos, bool no_lim)
 
 // Surface-gradient term max(eta1+Hm,0) - max(eta0+Hm,0) with Hm = min(D0,D1),
 // evaluated as eta1 - eta0 whenever both sides are wet at the lower bed so that
-// FP32 does not lose the wave to the depth's magnitude.
+// FP32 does not lose the wave to the depth's magnitude.  With h0, h1 > |D1 - D0|
+// both sides are (eta1 + Hm >= h1 - |D1 - D0| and eta0 + Hm >= h0 - |D1 - D0|),
+// and the term is eta1 - eta0 without the tests.
 __device__ __forceinline__ float surface_jump(float e0, float e1, float D0, float D1)
 {
     float Hm = fmin_(D0, D1);

@@ -215,12 +215,50 @@ __global__ void __launch_bounds__(kControllerThreads) controller_kernel(const Sc
     (void)nslots;
 }
 
+// Per unit: the largest still-water depth step |dep1 - dep0| over the edges
+// of its cells (ScenarioDev::unit_gmax), one block per unit.
+constexpr int kGmaxThreads = 128;
+__global__ void __launch_bounds__(kGmaxThreads) unit_gmax_kernel(ScenarioDev s, int nunits)
+{
+    const int u = blockIdx.x;
+    if (u >= nunits) return;
+    const int uy = u / s.tiles_x, tx = u - uy * s.tiles_x;
+    const int x0 = s.x_org + tx * kTileX, yb = uy * kHalfRows;
+    const size_t pitch = (size_t)s.pitch;
+    float m = 0.f;
+    // x edges between columns x-1 and x, x = x0 .. x0 + kTileX, of the unit's rows
+    for (int k = threadIdx.x; k < (kTileX + 1) * kHalfRows; k += blockDim.x) {
+        const int y = yb + k / (kTileX + 1), x = x0 + k % (kTileX + 1);
+        if (x >= 1 && x < s.nx && y < s.ny) m = fmaxf(m, fabsf(s.dep[y * pitch + x] - s.dep[y * pitch + x - 1]));
+    }
+    // y edges between rows y-1 and y, y = yb .. yb + kHalfRows, of the unit's columns
+    for (int k = threadIdx.x; k < (kHalfRows + 1) * kTileX; k += blockDim.x) {
+        const int y = yb + k / kTileX, x = x0 + k % kTileX;
+        if (x >= 0 && x < s.nx && y >= 1 && y < s.ny) m = fmaxf(m, fabsf(s.dep[y * pitch + x] - s.dep[(y - 1) * pitch + x]));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    __shared__ float w[kGmaxThreads / 32];
+    if ((threadIdx.x & 31) == 0) w[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int k = 1; k < kGmaxThreads / 32; k++) m = fmaxf(m, w[k]);
+        s.unit_gmax[u] = fmaxf(m, w[0]);
+    }
+}
+
+void launch_unit_gmax(const ScenarioDev *s_host, cudaStream_t st)
+{
+    const int nunits = s_host->tiles_x * ((s_host->ny + kHalfRows - 1) / kHalfRows);
+    if (nunits > 0) unit_gmax_kernel<<<nunits, kGmaxThreads, 0, st>>>(*s_host, nunits);
+}
+
 cudaError_t preload_output_kernels()
 {
     cudaFuncAttributes a;
     cudaError_t e;
     if ((e = cudaFuncGetAttributes(&a, controller_kernel)) || (e = cudaFuncGetAttributes(&a, init_state_kernel)) ||
-        (e = cudaFuncGetAttributes(&a, extract_kernel)) || (e = cudaFuncGetAttributes(&a, gauges_kernel)))
+        (e = cudaFuncGetAttributes(&a, extract_kernel)) || (e = cudaFuncGetAttributes(&a, gauges_kernel)) ||
+        (e = cudaFuncGetAttributes(&a, unit_gmax_kernel)))
         return e;
     return cudaSuccess;
 }

@@ -97,6 +97,9 @@ void launch_initial_dt(const StepLaunch &L, cudaStream_t st);
 void launch_lists_current(const StepLaunch &L, cudaStream_t st);
 // init_extract.cu: the step controller of every slot (launch 5 of a step)
 void launch_controller(const StepLaunch &L, cudaStream_t st);
+// init_extract.cu: per-unit depth steps (ScenarioDev::unit_gmax), after the
+// depths change
+void launch_unit_gmax(const ScenarioDev *s_host, cudaStream_t st);
 // init_extract.cu / okada.cu: load their kernels now rather than at first use
 cudaError_t preload_output_kernels();
 cudaError_t preload_okada_kernels();

@@ -40,6 +40,7 @@
 #include "kernels.h"
 
 #include <algorithm>
+#include <type_traits>
 #include <cfloat>
 
 namespace thy {
@@ -226,7 +227,9 @@ __device__ __forceinline__ void y_edge(const ScenarioDev &s, const Cell &m, cons
 __device__ __forceinline__ int units_y(const ScenarioDev &s) { return (s.ny + kHalfRows - 1) / kHalfRows; }
 
 // The geometric tests imply 1 <= tx <= tiles_x - 2 and 1 <= uy <= units_y - 2.
-__device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const UnitSum *__restrict__ sum, int tx, int uy)
+// *hmin: the smallest depth over the unit and its two-cell ring (when deep).
+__device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const UnitSum *__restrict__ sum, int tx, int uy,
+                                          float *hmin)
 {
     if (!s.tmap) return false;
     const int x0 = s.x_org + tx * kTileX, yb = uy * kHalfRows;
@@ -239,8 +242,18 @@ __device__ __forceinline__ bool unit_deep(const ScenarioDev &s, const UnitSum *_
     // together (a NaN, an unknown summary, fails its test as before)
     const float v0 = c->all.x, v1 = c[-1].R.x, v2 = c[1].L.x, v3 = c[-W].B.x, v4 = c[W].T.x;
     const float v5 = c[-W - 1].BR.x, v6 = c[-W + 1].BL.x, v7 = c[W - 1].TR.x, v8 = c[W + 1].TL.x;
+    *hmin = fminf(fminf(fminf(v0, v1), fminf(v2, v3)), fminf(fminf(v4, v5), fminf(fminf(v6, v7), v8)));
     return (v0 > hp) & (v1 > hp) & (v2 > hp) & (v3 > hp) & (v4 > hp) & (v5 > hp) & (v6 > hp) & (v7 > hp) & (v8 > hp);
 }
+
+// Deep-list entries: the unit code (2 x work-list index + half) and, in bit
+// kJumpPlain, whether every surface jump of the unit's edges in the state
+// the list was made for is the plain difference of the elevations (its unit
+// and ring deeper than unit_gmax, with a margin for the FP32 rounding of the
+// test itself).
+constexpr int kJumpPlain = 30;
+__device__ __forceinline__ int unit_code(int entry) { return entry & ((1 << kJumpPlain) - 1); }
+__device__ __forceinline__ bool jump_plain(int entry) { return (entry >> kJumpPlain) & 1; }
 
 // Outside the grid counts as dry (ghost cells copy the boundary cell), except
 // across a periodic x boundary, where the wrapped unit counts.
@@ -537,7 +550,7 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
     __shared__ int base2[2];                 // the block's first deep and general list slots
     for (int base = blockIdx.x * blockDim.x; base < n; base += gridDim.x * blockDim.x) {
         const int u = base + threadIdx.x;
-        bool listed = false, deep = false;
+        bool listed = false, deep = false, plain = false;
         ScenarioCtl *dry_ctl = nullptr;   // the scenario of a unit skipped as dry land this step
         if (u < n) {
             const int2 item = work[u >> 1];
@@ -550,8 +563,10 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
                 const bool running = !before_step && ctl->status == kRunning;
                 const int par = running ? (ctl->parity ^ 1) : ctl->parity;
                 const UnitSum *sum = s.usum[par];
-                deep = unit_deep(s, sum, tx, uy);
+                float hmin = 0.f;
+                deep = unit_deep(s, sum, tx, uy, &hmin);
                 const size_t k = (size_t)uy * s.tiles_x + tx;
+                plain = deep && hmin > 1.001f * s.unit_gmax[k] + 1e-6f;
                 int age = s.dry_age[k];
                 if (running) {
                     age = (!deep && unit_dry(s, sum, tx, uy)) ? min(age + 1, 255) : 0;
@@ -591,7 +606,7 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
         }
         const unsigned below = (1u << lane) - 1u;
         if (listed) {
-            if (deep) lists[2 + dbase + __popc(dm & below)] = u;
+            if (deep) lists[2 + dbase + __popc(dm & below)] = u | (plain ? 1 << kJumpPlain : 0);
             else lists[2 + cap + gbase + __popc(gm & below)] = u;
         }
         __syncthreads();   // cnt and base2 are reused by the next round
@@ -718,7 +733,17 @@ __device__ __forceinline__ void y_edge_deep(const ScenarioDev &s, const Cell &a,
     }
 }
 
+// surface jumps of two edges (e0 -> e1); PLAIN: the unit's depths exceed its
+// depth steps, so each is the plain difference (the same value)
+template <bool PLAIN>
+__device__ __forceinline__ float2 jump2(float2 e0, float2 e1, float2 D0, float2 D1)
+{
+    if (PLAIN) return sub2(e1, e0);
+    return make_float2(surface_jump(e0.x, e1.x, D0.x, D1.x), surface_jump(e0.y, e1.y, D0.y, D1.y));
+}
+
 // y edge of phase 2 between rows a (metrics ra) and b (rb) for two columns
+template <bool PLAIN>
 __device__ __forceinline__ void y_edge_deep2(const Cell2 &a, const Cell2 &b, float2 rha, float2 sha, float2 rhb,
                                              float2 shb, const DeepRow &ra, const DeepRow &rb, Contrib2 &lo,
                                              Contrib2 &hi)
@@ -727,7 +752,7 @@ __device__ __forceinline__ void y_edge_deep2(const Cell2 &a, const Cell2 &b, flo
     k.len = rb.y0.x; k.cmid = rb.y0.y; k.cdiff = rb.y0.z; k.c10 = rb.y0.w;
     k.c01 = rb.y1.x; k.li0 = rb.y1.y; k.kdes0 = rb.y1.z; k.kdes1 = rb.y1.w;
     k.cos0 = ra.m.x; k.cos1 = rb.m.x;
-    const float2 jump = make_float2(surface_jump(a.e.x, b.e.x, a.D.x, b.D.x), surface_jump(a.e.y, b.e.y, a.D.y, b.D.y));
+    const float2 jump = jump2<PLAIN>(a.e, b.e, a.D, b.D);
     MomFlux2 f;
     momentum_2s_y2(f, a.h, b.h, rha, rhb, sha, shb, a.qy, b.qy, a.qx, b.qx, jump, k);
     lo = {neg2(f.m_x), neg2(f.m_y), f.lam};
@@ -749,6 +774,7 @@ struct DeepUnit {
     float dt, t_sec, eps_h, dif_at, cfl, cvis;
     bool run;
     bool drop;                // test hook: issue no copy for it (its wait runs out)
+    bool plain;               // phase 2: every surface jump of the unit is the plain difference
 };
 static_assert(2 * sizeof(DeepUnit) + 16 <= kNextBytes, "claimed units' slots in shared memory");
 
@@ -757,7 +783,9 @@ __device__ __forceinline__ DeepUnit deep_unit(const ScenarioDev *__restrict__ sc
                                               const int *__restrict__ lists, int i)
 {
     DeepUnit d;
-    const int u = deep_items(lists)[i];
+    const int entry = deep_items(lists)[i];
+    const int u = unit_code(entry);
+    d.plain = jump_plain(entry);
     const int2 item = work[u >> 1];
     d.s = &scen[item.x];
     const int ty = item.y / d.s->tiles_x, tx = item.y - ty * d.s->tiles_x;
@@ -851,7 +879,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
     if (smem_addr(dsm) & 127u) {
         if (threadIdx.x == PT)
             for (int u = blockIdx.x; u < nunits; u += gridDim.x)
-                atomicOr(&scen[work[deep_items(lists)[u] >> 1].x].ctl->errors, 4u);
+                atomicOr(&scen[work[unit_code(deep_items(lists)[u]) >> 1].x].ctl->errors, 4u);
         return;
     }
     if (threadIdx.x == PT) {
@@ -1050,71 +1078,79 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 const int prow0 = PROWS * group2;
                 const int sc0 = strip2 * 56 + 2 + 2 * min(lane, 29);
                 const bool out_lane = (lane >= 1) && (lane <= 28);
-                const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
-                const int pitch = d.pitch;
-                const int r_first = prow0 + 1;                    // staged row of this warp's first output row
                 float local_max = -FLT_MAX;                        // max of lam / (2 cfl area)
-                int i = r_first * kStageW + sc0;
-                Cell2 c = staged_cell2(stage, i);
-                float2 rh_c = rcp_depth2(c.h), sh_c = sqrt2(c.h);
-                DeepRow rc = rows[r_first];
-                Contrib2 top;
-                {
-                    const Cell2 a = staged_cell2(stage, i - kStageW);
-                    Contrib2 dummy;
-                    y_edge_deep2(a, c, rcp_depth2(a.h), sqrt2(a.h), rh_c, sh_c, rows[r_first - 1], rc, dummy, top);
-                }
-                float *out0 = d.out0, *out1 = d.out1;
-                int off = (yb + r_first - 1) * pitch + x0 - 4 + sc0;
                 float2 fin = make_float2(0.f, 0.f);   // running sum: non-finite iff a new value is
-                // two rows an iteration, so that the row window is renamed
-                // rather than copied (every operation here is explicitly
-                // rounded: the copies compute alike)
-#pragma unroll 2
-                for (int k = 0; k < PROWS; k++, i += kStageW, off += pitch) {
-                    const DeepRow rn = rows[r_first + k + 1];
-                    const Cell2 n = staged_cell2(stage, i + kStageW);
-                    const float2 rh_n = rcp_depth2(n.h), sh_n = sqrt2(n.h);
-                    // y edges below this row
-                    Contrib2 below, next_top;
-                    y_edge_deep2(c, n, rh_c, sh_c, rh_n, sh_n, rc, rn, below, next_top);
-                    // x edges left of column sc0 (its left neighbour from shared
-                    // memory, 1/h and sqrt h from lane l-1) and between sc0 and sc0 + 1
-                    const float le = stage[i - 1], lD = stage[SPLANE + i - 1];
-                    const float lqx = stage[2 * SPLANE + i - 1], lqy = stage[3 * SPLANE + i - 1];
-                    const float rhL = shup(rh_c.y, 1), shL = shup(sh_c.y, 1);
-                    const float2 jump =
-                        make_float2(surface_jump(le, c.e.x, lD, c.D.x), surface_jump(c.e.x, c.e.y, c.D.x, c.D.y));
-                    MomFlux2 f;
-                    momentum_2s_x2(f, make_float2(le + lD, c.h.x), c.h, make_float2(rhL, rh_c.x), rh_c,
-                                   make_float2(shL, sh_c.x), sh_c, make_float2(lqx, c.qx.x), c.qx,
-                                   make_float2(lqy, c.qy.x), c.qy, jump, XRowK{rc.m.y, rc.kdx});
-                    // column sc0: right cell of the left edge, left cell of the
-                    // middle edge; column sc0 + 1: right cell of the middle edge,
-                    // left cell of lane l+1's left edge
-                    const Contrib2 xr = {neg2(f.p_x), neg2(f.p_y), f.lam};
-                    const Contrib2 xrr = {make_float2(-f.m_x.y, -shdn(f.m_x.x, 1)),
-                                          make_float2(-f.m_y.y, -shdn(f.m_y.x, 1)),
-                                          make_float2(f.lam.y, shdn(f.lam.x, 1))};
-                    // momentum update; the dt bound as in the scalar path
-                    const float2 lam = add2(add2(add2(xr.lam, xrr.lam), top.lam), below.lam);
-                    const float2 w = mul2(lam, bc2(rc.kcfl));
-                    const float wm = fmaxf(lam.x < kEps ? 0.f : w.x, lam.y < kEps ? 0.f : w.y);
-                    if (out_lane) local_max = fmaxf(local_max, wm);
-                    const float2 val = bc2(rc.dtA);
-                    const float2 qx = fma2(val, add2(add2(add2(xr.a, xrr.a), top.a), below.a), c.qx);
-                    const float2 qy = fma2(val, add2(add2(add2(xr.b, xrr.b), top.b), below.b), c.qy);
-                    if (out_lane) {
-                        fin = add2(fin, add2(qx, qy));
-                        *reinterpret_cast<float2 *>(out0 + off) = qx;
-                        *reinterpret_cast<float2 *>(out1 + off) = qy;
+                // the row loop in two copies: surface jumps with their wet/dry
+                // tests, or as plain differences (a unit the classification
+                // found deeper than its depth steps); a uniform branch per unit
+                auto pair_rows = [&](auto plain_tag) {
+                    constexpr bool PLAIN = decltype(plain_tag)::value;
+                    const float *stage = reinterpret_cast<const float *>(dsm + buf * SB);
+                    const int pitch = d.pitch;
+                    const int r_first = prow0 + 1;                    // staged row of this warp's first output row
+                    int i = r_first * kStageW + sc0;
+                    Cell2 c = staged_cell2(stage, i);
+                    float2 rh_c = rcp_depth2(c.h), sh_c = sqrt2(c.h);
+                    DeepRow rc = rows[r_first];
+                    Contrib2 top;
+                    {
+                        const Cell2 a = staged_cell2(stage, i - kStageW);
+                        Contrib2 dummy;
+                        y_edge_deep2<PLAIN>(a, c, rcp_depth2(a.h), sqrt2(a.h), rh_c, sh_c, rows[r_first - 1], rc, dummy, top);
                     }
-                    top = next_top;
-                    rc = rn;
-                    c = n;
-                    rh_c = rh_n;
-                    sh_c = sh_n;
-                }
+                    float *out0 = d.out0, *out1 = d.out1;
+                    int off = (yb + r_first - 1) * pitch + x0 - 4 + sc0;
+                    // two rows an iteration, so that the row window is renamed
+                    // rather than copied (every operation here is explicitly
+                    // rounded: the copies compute alike)
+    #pragma unroll 2
+                    for (int k = 0; k < PROWS; k++, i += kStageW, off += pitch) {
+                        const DeepRow rn = rows[r_first + k + 1];
+                        const Cell2 n = staged_cell2(stage, i + kStageW);
+                        const float2 rh_n = rcp_depth2(n.h), sh_n = sqrt2(n.h);
+                        // y edges below this row
+                        Contrib2 below, next_top;
+                        y_edge_deep2<PLAIN>(c, n, rh_c, sh_c, rh_n, sh_n, rc, rn, below, next_top);
+                        // x edges left of column sc0 (its left neighbour, with its 1/h
+                        // and sqrt h, is lane l-1's second column) and between sc0 and
+                        // sc0 + 1 (lane 0 is halo: its left edge is not used)
+                        const float le = shup(c.e.y, 1), lD = shup(c.D.y, 1);
+                        const float lqx = shup(c.qx.y, 1), lqy = shup(c.qy.y, 1);
+                        const float rhL = shup(rh_c.y, 1), shL = shup(sh_c.y, 1);
+                        const float2 jump = jump2<PLAIN>(make_float2(le, c.e.x), c.e, make_float2(lD, c.D.x), c.D);
+                        MomFlux2 f;
+                        momentum_2s_x2(f, make_float2(le + lD, c.h.x), c.h, make_float2(rhL, rh_c.x), rh_c,
+                                       make_float2(shL, sh_c.x), sh_c, make_float2(lqx, c.qx.x), c.qx,
+                                       make_float2(lqy, c.qy.x), c.qy, jump, XRowK{rc.m.y, rc.kdx});
+                        // column sc0: right cell of the left edge, left cell of the
+                        // middle edge; column sc0 + 1: right cell of the middle edge,
+                        // left cell of lane l+1's left edge
+                        const Contrib2 xr = {neg2(f.p_x), neg2(f.p_y), f.lam};
+                        const Contrib2 xrr = {make_float2(-f.m_x.y, -shdn(f.m_x.x, 1)),
+                                              make_float2(-f.m_y.y, -shdn(f.m_y.x, 1)),
+                                              make_float2(f.lam.y, shdn(f.lam.x, 1))};
+                        // momentum update; the dt bound as in the scalar path
+                        const float2 lam = add2(add2(add2(xr.lam, xrr.lam), top.lam), below.lam);
+                        const float2 w = mul2(lam, bc2(rc.kcfl));
+                        const float wm = fmaxf(lam.x < kEps ? 0.f : w.x, lam.y < kEps ? 0.f : w.y);
+                        if (out_lane) local_max = fmaxf(local_max, wm);
+                        const float2 val = bc2(rc.dtA);
+                        const float2 qx = fma2(val, add2(add2(add2(xr.a, xrr.a), top.a), below.a), c.qx);
+                        const float2 qy = fma2(val, add2(add2(add2(xr.b, xrr.b), top.b), below.b), c.qy);
+                        if (out_lane) {
+                            fin = add2(fin, add2(qx, qy));
+                            *reinterpret_cast<float2 *>(out0 + off) = qx;
+                            *reinterpret_cast<float2 *>(out1 + off) = qy;
+                        }
+                        top = next_top;
+                        rc = rn;
+                        c = n;
+                        rh_c = rh_n;
+                        sh_c = sh_n;
+                    }
+                };
+                if (d.plain) pair_rows(std::true_type{});
+                else pair_rows(std::false_type{});
                 if (!isfinite(fin.x) || !isfinite(fin.y)) atomicOr(&ctl->errors, 1u);
                 for (int o = 16; o > 0; o >>= 1) local_max = fmaxf(local_max, __shfl_xor_sync(0xffffffffu, local_max, o));
                 if (lane == 0) red[warp] = local_max;

@@ -141,7 +141,7 @@ size_t scenario_bytes(int nx, int ny, bool has_faults)
     size_t b = 10 * pitch * ny * sizeof(float);          // fields
     b += (size_t)(5 * ny + 1) * sizeof(float);           // row tables
     b += 3 * (size_t)nx * ny * sizeof(float);            // output staging
-    b += 2 * (size_t)((nx + 2 * kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(UnitSum) + 1);
+    b += 2 * (size_t)((nx + 2 * kTileX - 1) / kTileX) * ((ny + kTileY - 1) / kTileY) * (2 * sizeof(UnitSum) + 1 + sizeof(float));
     b += kNumMaps * sizeof(TmaMap) + (size_t)(ny + 1) * sizeof(float4);
     if (has_faults) b += (size_t)nx * ny * sizeof(double);
     return b + 4096 + kGaugeRing * sizeof(double);   // (gauges: 4 + 16 kGaugeRing + 8 bytes per point, not counted)
@@ -169,6 +169,7 @@ DevScenario::~DevScenario()
     if (fault_times_d) cudaFreeAsync(fault_times_d, ast);
     if (usum) cudaFreeAsync(usum, ast);
     if (dry_age) cudaFreeAsync(dry_age, ast);
+    if (gmax) cudaFreeAsync(gmax, ast);
     if (tmaps) cudaFreeAsync(tmaps, ast);
     if (rowpack) cudaFreeAsync(rowpack, ast);
 }
@@ -275,9 +276,11 @@ int DevScenario::setup(const thy_problem *p, cudaStream_t st)
     desc.ntiles = desc.tiles_x * desc.tiles_y;
     THY_CK(cudaMallocAsync(&usum, 4 * (size_t)desc.ntiles * sizeof(UnitSum), st));
     THY_CK(cudaMallocAsync(&dry_age, 2 * (size_t)desc.ntiles, st));
+    THY_CK(cudaMallocAsync(&gmax, 2 * (size_t)desc.ntiles * sizeof(float), st));
     desc.usum[0] = usum;
     desc.usum[1] = usum + 2 * desc.ntiles;
     desc.dry_age = dry_age;
+    desc.unit_gmax = gmax;
     desc.b_up = (float)p->border_up;
     desc.b_low = (float)p->border_low;
     desc.b_left = (float)p->border_left;
@@ -423,6 +426,11 @@ cudaError_t DevScenario::invalidate_tile_minima(cudaStream_t st)
 {
     cudaError_t e = cudaMemsetAsync(usum, 0xff, 4 * (size_t)desc.ntiles * sizeof(UnitSum), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(dry_age, 0, 2 * (size_t)desc.ntiles, st);
+    if (e == cudaSuccess) {
+        // the depths changed (set-up, a fault): their steps per unit again
+        launch_unit_gmax(&desc, st);
+        e = cudaGetLastError();
+    }
     return e;
 }
 
@@ -1376,6 +1384,10 @@ extern "C" int thy_run(const thy_problem *p, const thy_outputs *o, thy_stats *st
         if ((rc = s.setup(p, st))) goto out;
         s.desc.ctl = s.ctl;
         if ((rc = b.rebuild())) goto out;
+        // the delivery of snapshots and gauge samples (writer thread,
+        // page-locked slots, copy stream) is set up before the loop, as the
+        // reference creates its output files before its loop
+        if ((rc = s.open_outputs(o, st))) goto out;
         t0 = std::chrono::steady_clock::now();
         if (stats) stats->setup_seconds = std::chrono::duration<double>(t0 - t_start).count();
         if ((rc = initial_dt(b))) goto out;

@@ -54,6 +54,7 @@ struct DevScenario {
     double *fault_times_d = nullptr;
     UnitSum *usum = nullptr;       // 2 parities x 2 ntiles unit depth summaries (desc.usum)
     unsigned char *dry_age = nullptr;   // 2 ntiles (desc.dry_age)
+    float *gmax = nullptr;              // 2 ntiles depth steps per unit (desc.unit_gmax)
     TmaMap *tmaps = nullptr;       // kNumMaps tensor maps of the field planes (desc.tmap)
     float4 *rowpack = nullptr;     // ny+1 packed row metrics (desc.rowpack)
     ScenarioCtl *ctl = nullptr;    // device control block (owned by the batch slot)
