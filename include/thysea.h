@@ -274,7 +274,8 @@ typedef struct thy_server_opts {
     long long chunk_cells;        /* cells stepped per chunk: the resident scenario submitted first,
                                      then those with the least remaining work (cells x remaining
                                      steps), until their cells reach this (0: 2^24, one 4096^2 grid;
-                                     < 0: all) */
+                                     < 0: all); a scenario of at least half this many cells is
+                                     stepped only when submitted first, and then alone */
 } thy_server_opts;
 typedef struct thy_server_stats {
     long long submitted, admitted, completed, failed, cancelled, rejected;

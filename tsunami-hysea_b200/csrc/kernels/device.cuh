@@ -187,12 +187,30 @@ __host__ __device__ inline float fmin_(float a, float b) { return (b < a) ? b : 
 __device__ __forceinline__ float sgnf(float a) { return (a > 0.f) ? 1.f : ((a < 0.f) ? -1.f : 0.f); }
 __device__ __forceinline__ float pow4f(float a) { float b = a * a; return b * b; }
 
+// Approximate reciprocal square root and square root of the stepping
+// kernels.  The square root is x * rsqrt(x), an approximate reciprocal square
+// root and one multiply, written out so that every call site computes it
+// with the same two instructions: an approximate sqrtf is not lowered alike
+// at every site, and then two warp tilings of the same cells, which reach the
+// same formula through different code, differ in the last bit.
+// sqrt_ap(0) = 0; a negative or NaN argument gives NaN.
+__device__ __forceinline__ float rsqrt_ap(float x)
+{
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float sqrt_ap(float x)
+{
+    return x == 0.f ? 0.f : __fmul_rn(x, rsqrt_ap(x));
+}
+
 // Desingularised 1/h (src/GPU/Arista_kernel.cu:164): sqrt2 h / sqrt(h^4 + max(h,eps)^4),
 // which is exactly 1/h for h >= eps.
 __device__ __forceinline__ float inv_depth(float h, float eps)
 {
     if (h >= eps) return __frcp_rn(h);
-    return kSqrt2 * h * rsqrtf(pow4f(h) + pow4f(eps));
+    return kSqrt2 * h * rsqrt_ap(pow4f(h) + pow4f(eps));
 }
 
 // Monotone limiter of the WAF correction (src/GPU/Arista_kernel.cu:45-68).
@@ -360,7 +378,7 @@ __device__ __forceinline__ void momentum_2s_x(MomFlux &r, float h0, float h1, fl
     const float hij = 0.5f * (h0 + h1);
     const float u0n = u0 * rh0, u1n = u1 * rh1;
     const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
-    const float maxa = fabsf(uijn) + sqrtf(hij);
+    const float maxa = fabsf(uijn) + sqrt_ap(hij);
     float mx, my, px, py;
     if (uijn < 0.f) {
         mx = u1n * u1 * ilcos; px = -mx; mx += hij * jump * ilcos;
@@ -384,7 +402,7 @@ __device__ __forceinline__ void momentum_2s_y(MomFlux &r, float h0, float h1, fl
     const float hij = 0.5f * (h0 + h1);
     const float u0n = u0 * rh0, u1n = u1 * rh1;
     const float uijn = __fdividef(s0 * u0n + s1 * u1n, s0 + s1 + kEps);
-    const float maxa = fabsf(uijn) + sqrtf(hij);
+    const float maxa = fabsf(uijn) + sqrt_ap(hij);
     const float deta = k.cmid * jump - uijn * uijn * k.cdiff;
     float fym, fyp, fxm, fxp;
     if (uijn < 0.f) {
@@ -418,7 +436,7 @@ __device__ __forceinline__ float mass_flux(Edge &e, const ScenarioDev &s, float 
     if (!((h0 > kEps) || (h1 > kEps))) return 0.f;
     float q0n = e.u0 * e.normal, q1n = e.u1 * e.normal;
     const float hij = 0.5f * (h0 + h1);
-    const float c0 = sqrtf(hij);
+    const float c0 = sqrt_ap(hij);
     if ((h0 < s.eps_h) && (-e.e1 > e.D0)) q1n = 0.f;
     if ((h1 < s.eps_h) && (-e.e0 > e.D1)) q0n = 0.f;
     const float u0n = inv_depth(h0, s.eps_h) * q0n;
@@ -426,7 +444,7 @@ __device__ __forceinline__ float mass_flux(Edge &e, const ScenarioDev &s, float 
     q0n = u0n * h0;
     q1n = u1n * h1;
     const float F2s = LAT ? e.len * q0n * e.cos0 * e.normal : e.len * q0n * e.normal;
-    const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+    const float s0 = sqrt_ap(h0), s1 = sqrt_ap(h1);
     const float uijn = (s0 * u0n + s1 * u1n) / (s0 + s1 + kEps);
     const float val = (2.f * e.len * dt) / (e.area0 + e.area1);
     const float aut1 = fmin_(uijn - c0, u0n - s0);
@@ -469,7 +487,7 @@ __device__ __forceinline__ MomFlux momentum_flux_x(Edge &e, const ScenarioDev &s
     r.active = true;
     const float ilcos = e.len;
     if (all_deep(e, s.hpos)) {
-        momentum_2s_x(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrtf(e.h0), sqrtf(e.h1), e.u0, e.u1, e.v0,
+        momentum_2s_x(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrt_ap(e.h0), sqrt_ap(e.h1), e.u0, e.u1, e.v0,
                       e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1), make_xrow(ilcos, e.area0 + e.area1, dt, s.cvis));
         return r;
     }
@@ -484,10 +502,10 @@ __device__ __forceinline__ MomFlux momentum_flux_x(Edge &e, const ScenarioDev &s
     float u0n = h0rg * w0, u1n = h1rg * w1;
     w0 = u0n * h0;
     w1 = u1n * h1;
-    const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+    const float s0 = sqrt_ap(h0), s1 = sqrt_ap(h1);
     float uijn = (s0 * u0n + s1 * u1n) / (s0 + s1 + kEps);
     const float val = (2.f * ilcos * dt) / (e.area0 + e.area1);
-    const float c0 = sqrtf(hij);
+    const float c0 = sqrt_ap(hij);
     const float aut1 = fmin_(uijn - c0, u0n - s0);
     const float aut2 = fmax_(uijn + c0, u1n + s1);
     float maxa = fmax_(fabsf(aut2), fabsf(aut1));
@@ -560,7 +578,7 @@ __device__ __forceinline__ MomFlux momentum_flux_y(Edge &e, const ScenarioDev &s
     r.active = true;
     const float len = e.len;
     if (all_deep(e, s.hpos)) {
-        momentum_2s_y(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrtf(e.h0), sqrtf(e.h1), e.u0, e.u1, e.v0,
+        momentum_2s_y(r, e.h0, e.h1, rcp_depth(e.h0), rcp_depth(e.h1), sqrt_ap(e.h0), sqrt_ap(e.h1), e.u0, e.u1, e.v0,
                       e.v1, surface_jump(e.e0, e.e1, e.D0, e.D1),
                       make_yrow(e.cos0, e.cos1, __frcp_rn(e.cos0), __frcp_rn(e.cos1), len, e.area0 + e.area1, dt,
                                 s.cvis));
@@ -572,12 +590,12 @@ __device__ __forceinline__ MomFlux momentum_flux_y(Edge &e, const ScenarioDev &s
     const float icos0 = __frcp_rn(e.cos0), icos1 = __frcp_rn(e.cos1);
     float w0 = e.u0 * e.normal, w1 = e.u1 * e.normal;
     const float hij = 0.5f * (h0 + h1);
-    const float c0 = sqrtf(hij);
+    const float c0 = sqrt_ap(hij);
     if ((h0 < s.eps_h) && (-e.e1 > e.D0)) w1 = 0.f;
     if ((h1 < s.eps_h) && (-e.e0 > e.D1)) w0 = 0.f;
     const float h0rg = inv_depth(h0, s.eps_h), h1rg = inv_depth(h1, s.eps_h);
     float u0n = h0rg * w0, u1n = h1rg * w1;
-    const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+    const float s0 = sqrt_ap(h0), s1 = sqrt_ap(h1);
     float uijn = (s0 * u0n + s1 * u1n) / (s0 + s1 + kEps);
     const float val = (2.f * len * dt) / (e.area0 + e.area1);
     const float aut1 = fmin_(uijn - c0, u0n - s0);

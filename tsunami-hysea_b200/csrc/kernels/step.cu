@@ -143,9 +143,9 @@ __device__ __forceinline__ float initial_speed(Edge &e, const ScenarioDev &s)
     const float w0 = e.u0 * e.normal, w1 = e.u1 * e.normal;
     const float h0 = e.h0, h1 = e.h1, hij = 0.5f * (h0 + h1);
     const float u0n = inv_depth(h0, s.eps_h) * w0, u1n = inv_depth(h1, s.eps_h) * w1;
-    const float s0 = sqrtf(h0), s1 = sqrtf(h1);
+    const float s0 = sqrt_ap(h0), s1 = sqrt_ap(h1);
     const float uij = (s0 * u0n + s1 * u1n) / (s0 + s1 + kEps);
-    float maxa = fabsf(uij) + sqrtf(hij);
+    float maxa = fabsf(uij) + sqrt_ap(hij);
     if (maxa < s.eps_h) maxa += s.eps_h;
     return e.len * maxa;
 }
@@ -631,7 +631,7 @@ __device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b)
     return make_float2(px ? a.x : b.x, py ? a.y : b.y);
 }
 __device__ __forceinline__ float2 rcp_depth2(float2 h) { return make_float2(rcp_depth(h.x), rcp_depth(h.y)); }
-__device__ __forceinline__ float2 sqrt2(float2 h) { return make_float2(sqrtf(h.x), sqrtf(h.y)); }
+__device__ __forceinline__ float2 sqrt2(float2 h) { return make_float2(sqrt_ap(h.x), sqrt_ap(h.y)); }
 
 // two cells of a staged row (columns i, i + 1; i even)
 struct Cell2 {
@@ -970,7 +970,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 float rh_c = 0.f, sh_c = 0.f;
                 if (PHASE == 2) {
                     rh_c = rcp_depth(c.h);
-                    sh_c = sqrtf(c.h);
+                    sh_c = sqrt_ap(c.h);
                 }
                 DeepRow rc = row(r_first);
                 Contrib top;
@@ -979,7 +979,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     float rh_a = 0.f, sh_a = 0.f;
                     if (PHASE == 2) {
                         rh_a = rcp_depth(a.h);
-                        sh_a = sqrtf(a.h);
+                        sh_a = sqrt_ap(a.h);
                     }
                     Contrib dummy;
                     y_edge_deep<PHASE>(s, a, c, rh_a, sh_a, rh_c, sh_c, row(r_first - 1), rc, dt, dummy, top);
@@ -996,7 +996,7 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     float rh_n = 0.f, sh_n = 0.f;
                     if (PHASE == 2) {
                         rh_n = rcp_depth(n.h);
-                        sh_n = sqrtf(n.h);
+                        sh_n = sqrt_ap(n.h);
                     }
                     // y edge below this row
                     Contrib below, next_top;
@@ -1427,14 +1427,14 @@ __global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__res
                             const float fac = inv_depth(h, s.eps_h);
                             if (s.vmax > 0.f) {
                                 float ux = fac * qx, uy = fac * qy;
-                                const float uu = sqrtf(ux * ux + uy * uy);
+                                const float uu = sqrt_ap(ux * ux + uy * uy);
                                 if (uu > s.vmax) { ux *= s.vmax / uu; uy *= s.vmax / uu; }
                                 qx = ux * h;
                                 qy = uy * h;
                             }
                             // semi-implicit Manning friction with the pre-update speed (disImplicita)
                             const float u1x = fac * qx, u1y = fac * qy;
-                            const float u1 = sqrtf(qx_old * qx_old + qy_old * qy_old) * fac;
+                            const float u1 = sqrt_ap(qx_old * qx_old + qy_old * qy_old) * fac;
                             if (h > 0.f) {
                                 const float c1 = dt * s.mf0 * fabsf(u1) / (exp2f(log2f(h) * (4.f / 3.f)) + kEps);
                                 const float fr = h / (1.f + c1);

@@ -251,12 +251,12 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
         }
         any_running = true;
     }
-    // Work budget of the chunk: the resident scenarios with the least
-    // remaining work (cells x remaining steps at the current dt) are stepped
-    // until their cells reach chunk_cells; the others wait (status idle on
-    // the device, and their tiles are not on the chunk's work list).  Small
-    // requests are batched, a large one runs nearly alone, and no request's
-    // arithmetic changes.
+    // Work budget of the chunk: the resident scenario submitted first, then
+    // those with the least remaining work (cells x remaining steps at the
+    // current dt), are stepped until their cells reach chunk_cells; the
+    // others wait (status idle on the device, and their tiles are not on the
+    // chunk's work list).  Small requests are batched, a large one runs
+    // alone, and no request's arithmetic changes.
     std::vector<char> sel(cap, 0);
     if (any_running) {
         // the request submitted first is always stepped (so that no request
@@ -278,12 +278,22 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             order.emplace_back(i == first ? -1.0 : cells * std::max(steps, 1.0), i);
         }
         std::sort(order.begin(), order.end());
+        // a large request (at least half the chunk's cells) is stepped only
+        // when it was submitted first, and then alone, so that it runs at its
+        // own speed as in first-come-first-served; smaller ones are batched
         double taken = 0.0;
+        const double big = S->chunk_cells < 0 ? 1e300 : 0.5 * (double)S->chunk_cells;
+        bool alone = false;
         for (const auto &e : order) {
             Active *a = S->slots[e.second];
             DevScenario &s = *a->s;
-            const bool step = S->chunk_cells < 0 || taken < (double)S->chunk_cells;
-            if (step) taken += (double)s.nx * s.ny;
+            const double cells = (double)s.nx * s.ny;
+            bool step = !alone && (S->chunk_cells < 0 || taken < (double)S->chunk_cells);
+            if (step && cells >= big) {
+                if (e.second == first) alone = true;
+                else step = false;
+            }
+            if (step) taken += cells;
             sel[e.second] = step ? 1 : 0;
             const int want = step ? kRunning : kIdle;
             if (s.hctl.status != want || a->deferred == step) {
