@@ -275,7 +275,8 @@ typedef struct thy_server_opts {
                                      then those with the least remaining work (cells x remaining
                                      steps), until their cells reach this (0: 2^24, one 4096^2 grid;
                                      < 0: all); a scenario of at least half this many cells is
-                                     stepped only when submitted first, and then alone */
+                                     stepped only when submitted first, and then alone, and
+                                     queued requests are admitted after it */
 } thy_server_opts;
 typedef struct thy_server_stats {
     long long submitted, admitted, completed, failed, cancelled, rejected;

@@ -575,6 +575,13 @@ __global__ void __launch_bounds__(kClassifyThreads) classify_kernel(const Scenar
                 if (age >= kDryAge) {
                     listed = false;
                     if (running) dry_ctl = ctl;
+                } else if (!deep) {
+                    // a general unit: the general kernel of the next phase 1
+                    // folds its summary into the other parity's entry, from
+                    // the empty value (nothing reads that entry before then)
+                    float2 *e = reinterpret_cast<float2 *>(&s.usum[par ^ 1][k]);
+#pragma unroll
+                    for (int f = 0; f < 9; f++) e[f] = make_float2(FLT_MAX, -FLT_MAX);
                 }
             }
         }
@@ -1200,303 +1207,389 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
     }
 }
 
-// General kernel, one work unit (half tile) per CTA iteration, 4 x NG warps
-// (4 column strips x NG row groups of kHalfRows / NG rows): phase 0 over every
-// unit of the work list, phases 1 and 2 over the general list of the step.
+// General kernel: units that are not deep water (boundaries, sponge layers,
+// coasts, wet/dry fronts).  A unit's work is split into tasks of one warp
+// each: column strip `strip` (28 output columns and a two-column halo on
+// each side) and row group `group` (kHalfRows / NG rows).  general_part runs
+// one task: it marches the group's rows and returns the lane's dt bound
+// (phases 0 / 2), depth summary (phase 1) and error flag; cell: the lane
+// holds one of the strip's output cells, gx_out its grid column.
 template <int PHASE, int NG>
-__global__ void __launch_bounds__(128 * NG) step_kernel(const ScenarioDev *__restrict__ scen, const int2 *__restrict__ work,
-                                                   const int *__restrict__ nwork_ptr, const int *__restrict__ lists,
-                                                   int cap)
+__device__ __forceinline__ void general_part(const ScenarioDev &s, const ScenarioCtl *ctl, int tx, int uy, int strip,
+                                             int group, float &local_min, DepthAcc &hacc, bool &bad, bool &cell,
+                                             int &gx_out)
 {
-    constexpr int GWARPS = 4 * NG, GROWS = kHalfRows / NG;
+    constexpr int GROWS = kHalfRows / NG;
     static_assert(kHalfRows % NG == 0, "row groups of equal height");
-    __shared__ float red[GWARPS];          // phases 0 / 2: dt per warp
-    __shared__ float2 slots[9 * GWARPS];   // phase 1: unit summary per warp
+    const int lane = threadIdx.x & 31;
+    const int nx = s.nx, ny = s.ny;
+    const int uy0 = uy * kHalfRows;
+    const int unit_end = min(uy0 + kHalfRows, ny);
+    // this warp: column strip `strip`, rows y0 .. y_end-1 of the unit
+    const int x0 = s.x_org + tx * kTileX + strip * OUTW, y0 = uy0 + group * GROWS;
+    const int p = ctl->parity;
+    const float dt = (float)ctl->dt;
+    const float t_sec = (float)(ctl->t * ctl->T);
+    const int gx = x0 - 2 + lane;
+    const int col = map_col(gx, nx, s.periodic);
+    const bool has_edge = (lane >= 2) && (lane <= 30) && (gx >= 0) && (gx <= nx);
+    const bool has_cell = (lane >= 2) && (lane <= 29) && (gx >= 0) && (gx < nx);
+    const int y_end = min(y0 + GROWS, unit_end);
+    const float *eta_in = (PHASE == 2) ? s.eta[p ^ 1] : s.eta[p];
+    const float *qx_in = s.qx[p], *qy_in = s.qy[p];
+    const size_t pitch = (size_t)s.pitch;
+    const bool x_ghost_lo = !s.periodic && gx == 0, x_ghost_hi = !s.periodic && gx == nx;
+    const bool x_nolim = (gx < 2) || (gx > nx - 2);
+    const bool sponge = (s.sp_left | s.sp_right | s.sp_up | s.sp_low) != 0;
+    local_min = FLT_MAX;
+    hacc.init();
+    bad = false;
+    gx_out = gx;
+    cell = has_cell && x0 < nx && x0 + OUTW > 0;
+
+    if (x0 < nx && x0 + OUTW > 0 && y0 < y_end) {
+        constexpr bool DIAG = (PHASE == 1);
+        Cell c0 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 2, ny) * pitch + col);
+        Cell c1 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 1, ny) * pitch + col);
+        Cell c2, c3, c4;
+        {
+            // rows y0 .. y0+2 with their diagnostics (rows below the grid are clamped and skipped)
+            const RawCell r0 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0, ny) * pitch + col, has_cell);
+            const RawCell r1 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 1, ny) * pitch + col,
+                                              has_cell && y0 + 1 < y_end);
+            const RawCell r2 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 2, ny) * pitch + col,
+                                              has_cell && y0 + 2 < y_end);
+            if (DIAG && has_cell) {
+                diagnostics(s, r0, (size_t)y0 * pitch + col, t_sec);
+                if (y0 + 1 < y_end) diagnostics(s, r1, (size_t)(y0 + 1) * pitch + col, t_sec);
+                if (y0 + 2 < y_end) diagnostics(s, r2, (size_t)(y0 + 2) * pitch + col, t_sec);
+            }
+            c2 = finish(r0);
+            c3 = finish(r1);
+            c4 = finish(r2);
+        }
+        RawCell n1 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 3, ny) * pitch + col,
+                                    has_cell && y0 + 3 < y_end);
+        // y edge at the top of the first row (stencil rows y0-2 .. y0+1)
+        // row metrics {cos, ilcos, area, dlon} (rowpack), loaded a row
+        // ahead: kc of row yo, kn of row yo+1 (entry ny: dlon only)
+        const float4 *__restrict__ rp = s.rowpack;
+        float4 kc = __ldg(rp + y0);
+        float4 kn = __ldg(rp + y0 + 1);
+        Contrib top, dummy;
+        y_edge<PHASE>(s, c0, c1, c2, c3, y0, dt, dummy, top, __ldg(rp + clamp_row(y0 - 1, ny)), kc, kc.w);
+
+        for (int yo = y0; yo < y_end; yo++) {
+            const float4 knn = __ldg(rp + min(yo + 2, ny));
+            // rows yo+3 (loaded an iteration ago) and yo+4 (now) are in flight
+            const RawCell n2 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(yo + 4, ny) * pitch + col,
+                                              has_cell && yo + 4 < y_end);
+            const size_t idx = (size_t)yo * pitch + col;
+            // ---- y edge below this row (between yo and yo+1) ----
+            Contrib below, next_top;
+            y_edge<PHASE>(s, c1, c2, c3, c4, yo + 1, dt, below, next_top, kc, (yo + 1 < ny) ? kn : kc, kn.w);
+
+            // ---- x edge left of this lane's cell (row yo) ----
+            Edge e;
+            e.h0m = shup(c2.h, 2);
+            e.e0m = shup(c2.e, 2);
+            e.h0 = shup(c2.h, 1);
+            e.u0 = shup(c2.qx, 1);
+            e.h1 = c2.h;
+            e.u1 = c2.qx;
+            if (PHASE != 0) {
+                e.e0 = shup(c2.e, 1);
+                e.D0 = shup(c2.D, 1);
+                e.h1p = shdn(c2.h, 1);
+                e.e1p = shdn(c2.e, 1);
+                e.e1 = c2.e;
+                e.D1 = c2.D;
+            }
+            if (PHASE == 2) {
+                // the tangential discharge only enters the momentum flux
+                e.v0m = shup(c2.qy, 2);
+                e.v0 = shup(c2.qy, 1);
+                e.v1p = shdn(c2.qy, 1);
+                e.v1 = c2.qy;
+            } else {
+                e.v0m = e.v0 = e.v1p = e.v1 = 0.f;
+            }
+            e.u0m = e.u1p = 0.f;
+            const float area = kc.z;
+            e.area0 = e.area1 = area;
+            e.cos0 = e.cos1 = kc.x;
+            e.len = kc.y;
+            e.normal = 1.f;
+            e.front = false;
+            if (x_ghost_lo) {
+                e.u0 *= s.b_left;
+                e.normal = -1.f;
+                e.front = true;
+            }
+            if (x_ghost_hi) e.u1 *= s.b_right;
+            e.no_lim = x_nolim;
+            Contrib xl = {0.f, 0.f, 0.f}, xr = {0.f, 0.f, 0.f};
+            if (has_edge) {
+                if (PHASE == 1) {
+                    const float F = mass_flux<false>(e, s, dt);
+                    xl = {-F, 0.f, 0.f};
+                    xr = x_ghost_lo ? Contrib{-F, 0.f, 0.f} : Contrib{F, 0.f, 0.f};
+                } else if (PHASE == 2) {
+                    MomFlux f = momentum_flux_x(e, s, dt);
+                    if (!f.active) { f.m_x = f.m_y = f.p_x = f.p_y = f.lam = 0.f; }
+                    xl = {-f.m_x, -f.m_y, f.lam};
+                    xr = x_ghost_lo ? xl : Contrib{-f.p_x, -f.p_y, f.lam};
+                } else {
+                    const float lam = initial_speed(e, s);
+                    xl = {0.f, 0.f, lam};
+                    xr = xl;
+                }
+            }
+            // the right edge of this cell is the left edge of lane+1
+            Contrib xrr;
+            xrr.a = shdn(xl.a, 1);
+            if (PHASE == 2) xrr.b = shdn(xl.b, 1);
+            if (PHASE != 1) xrr.lam = shdn(xl.lam, 1);
+
+            // ---- cell (gx, yo) ----
+            if (has_cell) {
+                if (PHASE == 0) {
+                    const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
+                    const float step = (lam < kEps) ? 1e30f : __fdividef(2.f * s.cfl * area, lam);
+                    local_min = fminf(local_min, step);
+                } else if (PHASE == 1) {
+                    // mass update (src/GPU/Volumen_kernel.cu:111-157); the
+                    // diagnostics run when a row's loads complete
+                    const float acc = ((xr.a + xrr.a) + top.a) + below.a;
+                    const float D = c2.D;
+                    float eta = c2.e + __fdividef(dt, area) * acc;
+                    if (!(eta + D > 0.f)) eta = -D;
+                    if (sponge && ((gx < s.sp_left) || (gx >= nx - s.sp_right) || (yo < s.sp_up) ||
+                                   (yo >= ny - s.sp_low))) {
+                        const float dx = __ldg(s.row.dlon + yo), dy = __ldg(s.row.dlat + yo);
+                        float dl = (s.sp_left - gx - 0.5f) * dx, dr = (gx - (nx - 1 - s.sp_right) - 0.5f) * dx;
+                        float du = (s.sp_up - yo - 0.5f) * dy, dd = (yo - (ny - 1 - s.sp_low) - 0.5f) * dy;
+                        if (dl <= 0.f) dl = 1e30f;
+                        if (dr <= 0.f) dr = 1e30f;
+                        if (du <= 0.f) du = 1e30f;
+                        if (dd <= 0.f) dd = 1e30f;
+                        float dist, ls;
+                        if ((dl <= dr) && (dl <= du) && (dl <= dd)) { dist = dl; ls = dx * s.sp_left; }
+                        else if ((dr <= dl) && (dr <= du) && (dr <= dd)) { dist = dr; ls = dx * s.sp_right; }
+                        else if ((du <= dl) && (du <= dr) && (du <= dd)) { dist = du; ls = dy * s.sp_up; }
+                        else { dist = dd; ls = dy * s.sp_low; }
+                        const float rr = dist / ls, co = 0.9f * rr * rr;
+                        // relax h towards max(D + sea level, 0), expressed on eta
+                        const float eta_rest = (D + s.sea > 0.f) ? s.sea : -D;
+                        eta -= co * (eta - eta_rest);
+                        if (!(eta + D >= 0.f)) eta = -D;
+                    }
+                    if (!isfinite(eta)) bad = true;
+                    s.eta[p ^ 1][idx] = eta;
+                    hacc.add(eta + D, yo - uy0 < 2, unit_end - yo <= 2);
+                } else {
+                    // momentum update (src/GPU/Volumen_kernel.cu:175-219)
+                    const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
+                    const float step = (lam < kEps) ? 1e30f : __fdividef(2.f * s.cfl * area, lam);
+                    local_min = fminf(local_min, step);
+                    const float val = __fdividef(dt, area);
+                    const float qx_old = c2.qx, qy_old = c2.qy;
+                    float qx = qx_old + val * (((xr.a + xrr.a) + top.a) + below.a);
+                    float qy = qy_old + val * (((xr.b + xrr.b) + top.b) + below.b);
+                    const float h = c2.h;
+                    if (sponge) {
+                        const float dx = __ldg(s.row.dlon + yo), dy = __ldg(s.row.dlat + yo);
+                        if (gx < s.sp_left) {
+                            const float rr = ((s.sp_left - gx - 0.5f) * dx) / (dx * s.sp_left);
+                            qx -= 0.9f * rr * rr * qx;
+                        }
+                        if (gx >= nx - s.sp_right) {
+                            const float rr = ((gx - (nx - 1 - s.sp_right) - 0.5f) * dx) / (dx * s.sp_right);
+                            qx -= 0.9f * rr * rr * qx;
+                        }
+                        if (yo < s.sp_up) {
+                            const float rr = ((s.sp_up - yo - 0.5f) * dy) / (dy * s.sp_up);
+                            qy -= 0.9f * rr * rr * qy;
+                        }
+                        if (yo >= ny - s.sp_low) {
+                            const float rr = ((yo - (ny - 1 - s.sp_low) - 0.5f) * dy) / (dy * s.sp_low);
+                            qy -= 0.9f * rr * rr * qy;
+                        }
+                    }
+                    if (h <= s.hpos) {
+                        // damping of almost-dry cells and velocity cap (filtroEstado)
+                        const float f = h / s.eps_h;
+                        const float damp = __expf(-dt * (1.f / (pow4f(f) + kEps)));
+                        qx *= damp;
+                        qy *= damp;
+                        const float fac = inv_depth(h, s.eps_h);
+                        if (s.vmax > 0.f) {
+                            float ux = fac * qx, uy = fac * qy;
+                            const float uu = sqrt_ap(ux * ux + uy * uy);
+                            if (uu > s.vmax) { ux *= s.vmax / uu; uy *= s.vmax / uu; }
+                            qx = ux * h;
+                            qy = uy * h;
+                        }
+                        // semi-implicit Manning friction with the pre-update speed (disImplicita)
+                        const float u1x = fac * qx, u1y = fac * qy;
+                        const float u1 = sqrt_ap(qx_old * qx_old + qy_old * qy_old) * fac;
+                        if (h > 0.f) {
+                            const float c1 = dt * s.mf0 * fabsf(u1) / (exp2f(log2f(h) * (4.f / 3.f)) + kEps);
+                            const float fr = h / (1.f + c1);
+                            qx = fr * u1x;
+                            qy = fr * u1y;
+                        }
+                    }
+                    if (!isfinite(qx) || !isfinite(qy)) bad = true;
+                    s.qx[p ^ 1][idx] = qx;
+                    s.qy[p ^ 1][idx] = qy;
+                }
+            }
+            top = next_top;
+            kc = kn;
+            kn = knn;
+            c0 = c1;
+            c1 = c2;
+            c2 = c3;
+            c3 = c4;
+            if (DIAG && has_cell && yo + 3 < y_end) diagnostics(s, n1, idx + 3 * pitch, t_sec);
+            c4 = finish(n1);
+            n1 = n2;
+        }
+    }
+}
+
+// Phase 0 (the initial dt) over every unit of the work list, one unit per CTA
+// iteration, 4 x NG warps; the last unit of a scenario stores its dt.
+template <int NG>
+__global__ void __launch_bounds__(128 * NG) initial_dt_kernel(const ScenarioDev *__restrict__ scen,
+                                                              const int2 *__restrict__ work,
+                                                              const int *__restrict__ nwork_ptr)
+{
+    constexpr int GWARPS = 4 * NG;
+    __shared__ float red[GWARPS];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int strip = warp % STRIPS, group = warp / STRIPS;
-    const int nitems = (PHASE == 0) ? 2 * *nwork_ptr : lists[1];
-    for (int g = blockIdx.x; g < nitems; g += gridDim.x) {
-        const int u = (PHASE == 0) ? g : general_items(lists, cap)[g];
+    const int nitems = 2 * *nwork_ptr;
+    for (int u = blockIdx.x; u < nitems; u += gridDim.x) {
         const int2 item = work[u >> 1];
         const ScenarioDev &s = scen[item.x];
         ScenarioCtl *ctl = s.ctl;
-        const int status = *((volatile int *)&ctl->status);
-        if (PHASE != 0 && status != kRunning) continue;
-        const int nx = s.nx, ny = s.ny;
         const int ty = item.y / s.tiles_x, tx = item.y - ty * s.tiles_x;
         const int uy = 2 * ty + (u & 1);
-        const int uy0 = uy * kHalfRows;
-        if (uy0 >= ny) continue;   // a unit below the grid (phase 0 only; never listed)
-        const int unit_end = min(uy0 + kHalfRows, ny);
-        // this warp: column strip `strip`, rows y0 .. y_end-1 of the unit
-        const int x0 = s.x_org + tx * kTileX + strip * OUTW, y0 = uy0 + group * GROWS;
-        const int p = ctl->parity;
-        const float dt = (float)ctl->dt;
-        const float t_sec = (float)(ctl->t * ctl->T);
-        const int gx = x0 - 2 + lane;
-        const int col = map_col(gx, nx, s.periodic);
-        const bool has_edge = (lane >= 2) && (lane <= 30) && (gx >= 0) && (gx <= nx);
-        const bool has_cell = (lane >= 2) && (lane <= 29) && (gx >= 0) && (gx < nx);
-        const int y_end = min(y0 + GROWS, unit_end);
-        const float *eta_in = (PHASE == 2) ? s.eta[p ^ 1] : s.eta[p];
-        const float *qx_in = s.qx[p], *qy_in = s.qy[p];
-        const size_t pitch = (size_t)s.pitch;
-        const bool x_ghost_lo = !s.periodic && gx == 0, x_ghost_hi = !s.periodic && gx == nx;
-        const bool x_nolim = (gx < 2) || (gx > nx - 2);
-        const bool sponge = (s.sp_left | s.sp_right | s.sp_up | s.sp_low) != 0;
-        float local_min = FLT_MAX;    // phases 0 / 2: dt
-        DepthAcc hacc;                // phase 1: depth summary
-        hacc.init();
-        bool bad = false;
-
-        if (x0 < nx && x0 + OUTW > 0 && y0 < y_end) {
-            constexpr bool DIAG = (PHASE == 1);
-            Cell c0 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 2, ny) * pitch + col);
-            Cell c1 = load_cell(eta_in, s.dep, qx_in, qy_in, clamp_row(y0 - 1, ny) * pitch + col);
-            Cell c2, c3, c4;
-            {
-                // rows y0 .. y0+2 with their diagnostics (rows below the grid are clamped and skipped)
-                const RawCell r0 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0, ny) * pitch + col, has_cell);
-                const RawCell r1 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 1, ny) * pitch + col,
-                                                  has_cell && y0 + 1 < y_end);
-                const RawCell r2 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 2, ny) * pitch + col,
-                                                  has_cell && y0 + 2 < y_end);
-                if (DIAG && has_cell) {
-                    diagnostics(s, r0, (size_t)y0 * pitch + col, t_sec);
-                    if (y0 + 1 < y_end) diagnostics(s, r1, (size_t)(y0 + 1) * pitch + col, t_sec);
-                    if (y0 + 2 < y_end) diagnostics(s, r2, (size_t)(y0 + 2) * pitch + col, t_sec);
-                }
-                c2 = finish(r0);
-                c3 = finish(r1);
-                c4 = finish(r2);
-            }
-            RawCell n1 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(y0 + 3, ny) * pitch + col,
-                                        has_cell && y0 + 3 < y_end);
-            // y edge at the top of the first row (stencil rows y0-2 .. y0+1)
-            // row metrics {cos, ilcos, area, dlon} (rowpack), loaded a row
-            // ahead: kc of row yo, kn of row yo+1 (entry ny: dlon only)
-            const float4 *__restrict__ rp = s.rowpack;
-            float4 kc = __ldg(rp + y0);
-            float4 kn = __ldg(rp + y0 + 1);
-            Contrib top, dummy;
-            y_edge<PHASE>(s, c0, c1, c2, c3, y0, dt, dummy, top, __ldg(rp + clamp_row(y0 - 1, ny)), kc, kc.w);
-
-            for (int yo = y0; yo < y_end; yo++) {
-                const float4 knn = __ldg(rp + min(yo + 2, ny));
-                // rows yo+3 (loaded an iteration ago) and yo+4 (now) are in flight
-                const RawCell n2 = load_raw<DIAG>(s, eta_in, qx_in, qy_in, clamp_row(yo + 4, ny) * pitch + col,
-                                                  has_cell && yo + 4 < y_end);
-                const size_t idx = (size_t)yo * pitch + col;
-                // ---- y edge below this row (between yo and yo+1) ----
-                Contrib below, next_top;
-                y_edge<PHASE>(s, c1, c2, c3, c4, yo + 1, dt, below, next_top, kc, (yo + 1 < ny) ? kn : kc, kn.w);
-
-                // ---- x edge left of this lane's cell (row yo) ----
-                Edge e;
-                e.h0m = shup(c2.h, 2);
-                e.e0m = shup(c2.e, 2);
-                e.h0 = shup(c2.h, 1);
-                e.u0 = shup(c2.qx, 1);
-                e.h1 = c2.h;
-                e.u1 = c2.qx;
-                if (PHASE != 0) {
-                    e.e0 = shup(c2.e, 1);
-                    e.D0 = shup(c2.D, 1);
-                    e.h1p = shdn(c2.h, 1);
-                    e.e1p = shdn(c2.e, 1);
-                    e.e1 = c2.e;
-                    e.D1 = c2.D;
-                }
-                if (PHASE == 2) {
-                    // the tangential discharge only enters the momentum flux
-                    e.v0m = shup(c2.qy, 2);
-                    e.v0 = shup(c2.qy, 1);
-                    e.v1p = shdn(c2.qy, 1);
-                    e.v1 = c2.qy;
-                } else {
-                    e.v0m = e.v0 = e.v1p = e.v1 = 0.f;
-                }
-                e.u0m = e.u1p = 0.f;
-                const float area = kc.z;
-                e.area0 = e.area1 = area;
-                e.cos0 = e.cos1 = kc.x;
-                e.len = kc.y;
-                e.normal = 1.f;
-                e.front = false;
-                if (x_ghost_lo) {
-                    e.u0 *= s.b_left;
-                    e.normal = -1.f;
-                    e.front = true;
-                }
-                if (x_ghost_hi) e.u1 *= s.b_right;
-                e.no_lim = x_nolim;
-                Contrib xl = {0.f, 0.f, 0.f}, xr = {0.f, 0.f, 0.f};
-                if (has_edge) {
-                    if (PHASE == 1) {
-                        const float F = mass_flux<false>(e, s, dt);
-                        xl = {-F, 0.f, 0.f};
-                        xr = x_ghost_lo ? Contrib{-F, 0.f, 0.f} : Contrib{F, 0.f, 0.f};
-                    } else if (PHASE == 2) {
-                        MomFlux f = momentum_flux_x(e, s, dt);
-                        if (!f.active) { f.m_x = f.m_y = f.p_x = f.p_y = f.lam = 0.f; }
-                        xl = {-f.m_x, -f.m_y, f.lam};
-                        xr = x_ghost_lo ? xl : Contrib{-f.p_x, -f.p_y, f.lam};
-                    } else {
-                        const float lam = initial_speed(e, s);
-                        xl = {0.f, 0.f, lam};
-                        xr = xl;
-                    }
-                }
-                // the right edge of this cell is the left edge of lane+1
-                Contrib xrr;
-                xrr.a = shdn(xl.a, 1);
-                if (PHASE == 2) xrr.b = shdn(xl.b, 1);
-                if (PHASE != 1) xrr.lam = shdn(xl.lam, 1);
-
-                // ---- cell (gx, yo) ----
-                if (has_cell) {
-                    if (PHASE == 0) {
-                        const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
-                        const float step = (lam < kEps) ? 1e30f : __fdividef(2.f * s.cfl * area, lam);
-                        local_min = fminf(local_min, step);
-                    } else if (PHASE == 1) {
-                        // mass update (src/GPU/Volumen_kernel.cu:111-157); the
-                        // diagnostics run when a row's loads complete
-                        const float acc = ((xr.a + xrr.a) + top.a) + below.a;
-                        const float D = c2.D;
-                        float eta = c2.e + __fdividef(dt, area) * acc;
-                        if (!(eta + D > 0.f)) eta = -D;
-                        if (sponge && ((gx < s.sp_left) || (gx >= nx - s.sp_right) || (yo < s.sp_up) ||
-                                       (yo >= ny - s.sp_low))) {
-                            const float dx = __ldg(s.row.dlon + yo), dy = __ldg(s.row.dlat + yo);
-                            float dl = (s.sp_left - gx - 0.5f) * dx, dr = (gx - (nx - 1 - s.sp_right) - 0.5f) * dx;
-                            float du = (s.sp_up - yo - 0.5f) * dy, dd = (yo - (ny - 1 - s.sp_low) - 0.5f) * dy;
-                            if (dl <= 0.f) dl = 1e30f;
-                            if (dr <= 0.f) dr = 1e30f;
-                            if (du <= 0.f) du = 1e30f;
-                            if (dd <= 0.f) dd = 1e30f;
-                            float dist, ls;
-                            if ((dl <= dr) && (dl <= du) && (dl <= dd)) { dist = dl; ls = dx * s.sp_left; }
-                            else if ((dr <= dl) && (dr <= du) && (dr <= dd)) { dist = dr; ls = dx * s.sp_right; }
-                            else if ((du <= dl) && (du <= dr) && (du <= dd)) { dist = du; ls = dy * s.sp_up; }
-                            else { dist = dd; ls = dy * s.sp_low; }
-                            const float rr = dist / ls, co = 0.9f * rr * rr;
-                            // relax h towards max(D + sea level, 0), expressed on eta
-                            const float eta_rest = (D + s.sea > 0.f) ? s.sea : -D;
-                            eta -= co * (eta - eta_rest);
-                            if (!(eta + D >= 0.f)) eta = -D;
-                        }
-                        if (!isfinite(eta)) bad = true;
-                        s.eta[p ^ 1][idx] = eta;
-                        hacc.add(eta + D, yo - uy0 < 2, unit_end - yo <= 2);
-                    } else {
-                        // momentum update (src/GPU/Volumen_kernel.cu:175-219)
-                        const float lam = ((xr.lam + xrr.lam) + top.lam) + below.lam;
-                        const float step = (lam < kEps) ? 1e30f : __fdividef(2.f * s.cfl * area, lam);
-                        local_min = fminf(local_min, step);
-                        const float val = __fdividef(dt, area);
-                        const float qx_old = c2.qx, qy_old = c2.qy;
-                        float qx = qx_old + val * (((xr.a + xrr.a) + top.a) + below.a);
-                        float qy = qy_old + val * (((xr.b + xrr.b) + top.b) + below.b);
-                        const float h = c2.h;
-                        if (sponge) {
-                            const float dx = __ldg(s.row.dlon + yo), dy = __ldg(s.row.dlat + yo);
-                            if (gx < s.sp_left) {
-                                const float rr = ((s.sp_left - gx - 0.5f) * dx) / (dx * s.sp_left);
-                                qx -= 0.9f * rr * rr * qx;
-                            }
-                            if (gx >= nx - s.sp_right) {
-                                const float rr = ((gx - (nx - 1 - s.sp_right) - 0.5f) * dx) / (dx * s.sp_right);
-                                qx -= 0.9f * rr * rr * qx;
-                            }
-                            if (yo < s.sp_up) {
-                                const float rr = ((s.sp_up - yo - 0.5f) * dy) / (dy * s.sp_up);
-                                qy -= 0.9f * rr * rr * qy;
-                            }
-                            if (yo >= ny - s.sp_low) {
-                                const float rr = ((yo - (ny - 1 - s.sp_low) - 0.5f) * dy) / (dy * s.sp_low);
-                                qy -= 0.9f * rr * rr * qy;
-                            }
-                        }
-                        if (h <= s.hpos) {
-                            // damping of almost-dry cells and velocity cap (filtroEstado)
-                            const float f = h / s.eps_h;
-                            const float damp = __expf(-dt * (1.f / (pow4f(f) + kEps)));
-                            qx *= damp;
-                            qy *= damp;
-                            const float fac = inv_depth(h, s.eps_h);
-                            if (s.vmax > 0.f) {
-                                float ux = fac * qx, uy = fac * qy;
-                                const float uu = sqrt_ap(ux * ux + uy * uy);
-                                if (uu > s.vmax) { ux *= s.vmax / uu; uy *= s.vmax / uu; }
-                                qx = ux * h;
-                                qy = uy * h;
-                            }
-                            // semi-implicit Manning friction with the pre-update speed (disImplicita)
-                            const float u1x = fac * qx, u1y = fac * qy;
-                            const float u1 = sqrt_ap(qx_old * qx_old + qy_old * qy_old) * fac;
-                            if (h > 0.f) {
-                                const float c1 = dt * s.mf0 * fabsf(u1) / (exp2f(log2f(h) * (4.f / 3.f)) + kEps);
-                                const float fr = h / (1.f + c1);
-                                qx = fr * u1x;
-                                qy = fr * u1y;
-                            }
-                        }
-                        if (!isfinite(qx) || !isfinite(qy)) bad = true;
-                        s.qx[p ^ 1][idx] = qx;
-                        s.qy[p ^ 1][idx] = qy;
-                    }
-                }
-                top = next_top;
-                kc = kn;
-                kn = knn;
-                c0 = c1;
-                c1 = c2;
-                c2 = c3;
-                c3 = c4;
-                if (DIAG && has_cell && yo + 3 < y_end) diagnostics(s, n1, idx + 3 * pitch, t_sec);
-                c4 = finish(n1);
-                n1 = n2;
-            }
-        }
+        if (uy * kHalfRows >= s.ny) continue;   // a unit below the grid (CTA-uniform)
+        float local_min;
+        DepthAcc hacc;
+        bool bad, cell;
+        int gx;
+        general_part<0, NG>(s, ctl, tx, uy, strip, group, local_min, hacc, bad, cell, gx);
         if (bad) atomicOr(&ctl->errors, 1u);
-
-        // ---- unit reductions: phase 1 depth summary -> usum; phase 0/2 dt -> scenario min ----
-        if (PHASE == 1) {
-            // the unit's first two and last two columns inside the grid
-            const int tx0 = s.x_org + tx * kTileX, ux0 = max(tx0, 0), ux1 = min(tx0 + kTileX, nx);
-            const bool cell = has_cell && x0 < nx && x0 + OUTW > 0;
-            warp_unit_summary(hacc, cell, cell && gx < ux0 + 2, cell && gx >= ux1 - 2, slots + 9 * warp);
-        } else {
-            for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
-            if (PHASE == 2) {
-                // one atomic per warp and no barrier: the minimum is exact in
-                // any order, and the warps of a CTA go on to their next unit
-                // without waiting for the slowest
-                if (lane == 0) atomicMin(&ctl->dt_bits, __float_as_uint(local_min));
-                continue;
-            }
-            if (lane == 0) red[warp] = local_min;
-        }
+        for (int o = 16; o > 0; o >>= 1) local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+        if (lane == 0) red[warp] = local_min;
         __syncthreads();
-        if (PHASE == 1) store_unit_summary(&s.usum[p ^ 1][(size_t)uy * s.tiles_x + tx], slots, GWARPS);
-        if (PHASE != 1 && threadIdx.x == 0) {
+        if (threadIdx.x == 0) {
             float m = red[0];
             for (int k = 1; k < GWARPS; k++) m = fminf(m, red[k]);
             atomicMin(&ctl->dt_bits, __float_as_uint(m));
-            if (PHASE == 0) {
-                // initial dt: the last tile stores the min and resets the counters
+            // the last unit stores the min and resets the counters
+            __threadfence();
+            const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
+            if (prev == (unsigned)(s.tiles_x * units_y(s) - 1)) {
                 __threadfence();
-                const unsigned prev = atomicAdd(&ctl->tiles_done, 1u);
-                if (prev == (unsigned)(s.tiles_x * units_y(s) - 1)) {
-                    __threadfence();
-                    ctl->dt = (double)__uint_as_float(atomicOr(&ctl->dt_bits, 0u));
-                    ctl->dt_bits = 0x7f7fffffu;
-                    ctl->tiles_done = 0u;
-                }
+                ctl->dt = (double)__uint_as_float(atomicOr(&ctl->dt_bits, 0u));
+                ctl->dt_bits = 0x7f7fffffu;
+                ctl->tiles_done = 0u;
             }
         }
-        __syncthreads();   // red[] is reused by the next item
+        __syncthreads();   // red[] is reused by the next unit
+    }
+}
+
+// Folds one warp's share of a unit's depth summary (nine {min, max}, UnitSum
+// order; a field the warp holds no cell of is left alone) into the unit's
+// summary with integer atomics on the float bits: depths are >= 0, where the
+// bit patterns order as the values do (a -0 counts as +0), and min and max are
+// exact in any order, so the summary does not depend on which warp came
+// first.  The classification resets the summaries of the general units it
+// lists to the empty value (FLT_MAX, -FLT_MAX) before this phase runs.
+__device__ __forceinline__ void fold_unit_summary(const DepthAcc &a, bool cell, bool is_l, bool is_r, UnitSum *dst)
+{
+    const float2 none = make_float2(FLT_MAX, -FLT_MAX);
+    const bool has_t = __any_sync(0xffffffffu, cell && a.tmin != FLT_MAX);
+    const bool has_b = __any_sync(0xffffffffu, cell && a.bmin != FLT_MAX);
+    const bool has_l = __any_sync(0xffffffffu, is_l), has_r = __any_sync(0xffffffffu, is_r);
+    float2 f[9];
+    f[0] = warp_minmax(a.amin, a.amax, cell);
+    f[1] = has_l ? warp_minmax(a.amin, a.amax, is_l) : none;
+    f[2] = has_r ? warp_minmax(a.amin, a.amax, is_r) : none;
+    f[3] = has_t ? warp_minmax(a.tmin, a.tmax, cell) : none;
+    f[4] = has_b ? warp_minmax(a.bmin, a.bmax, cell) : none;
+    f[5] = (has_l && has_t) ? warp_minmax(a.tmin, a.tmax, is_l) : none;
+    f[6] = (has_r && has_t) ? warp_minmax(a.tmin, a.tmax, is_r) : none;
+    f[7] = (has_l && has_b) ? warp_minmax(a.bmin, a.bmax, is_l) : none;
+    f[8] = (has_r && has_b) ? warp_minmax(a.bmin, a.bmax, is_r) : none;
+    if ((threadIdx.x & 31) == 0) {
+        int *d = reinterpret_cast<int *>(dst);
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            if (f[k].x == FLT_MAX) continue;   // no cell of this field in the task
+            const int lo = __float_as_int(f[k].x), hi = __float_as_int(f[k].y);
+            atomicMin(d + 2 * k, lo == (int)0x80000000 ? 0 : lo);
+            atomicMax(d + 2 * k + 1, hi == (int)0x80000000 ? 0 : hi);
+        }
+    }
+}
+
+// Phases 1 and 2 over the general list of the step.  Every warp runs tasks on
+// its own: the first wave takes tasks by warp index, then each warp claims
+// its next task from *claim (zeroed by the classification), so no warp waits
+// for another and a unit's strips outside the grid (in the first and last
+// tile columns) cost nothing.  The tasks of a unit are consecutive, so that
+// its strips and row groups run side by side and share their halo rows in L2.
+constexpr int kGeneralThreads = 128;
+template <int PHASE, int NG>
+__global__ void __launch_bounds__(kGeneralThreads, 4) general_kernel(const ScenarioDev *__restrict__ scen,
+                                                                    const int2 *__restrict__ work,
+                                                                    const int *__restrict__ lists, int cap,
+                                                                    int *__restrict__ claim)
+{
+    constexpr int TASKS = STRIPS * NG;   // tasks per unit
+    constexpr int WPB = kGeneralThreads / 32;
+    const int lane = threadIdx.x & 31;
+    const int ntasks = lists[1] * TASKS;
+    const int first_wave = (int)gridDim.x * WPB;
+    int t = blockIdx.x * WPB + (threadIdx.x >> 5);
+    while (t < ntasks) {
+        const int g = t / TASKS, r = t - g * TASKS;
+        const int group = r / STRIPS, strip = r - group * STRIPS;
+        const int u = general_items(lists, cap)[g];
+        const int2 item = work[u >> 1];
+        const ScenarioDev &s = scen[item.x];
+        ScenarioCtl *ctl = s.ctl;
+        if (*((volatile int *)&ctl->status) == kRunning) {
+            const int ty = item.y / s.tiles_x, tx = item.y - ty * s.tiles_x;
+            const int uy = 2 * ty + (u & 1);
+            float local_min;
+            DepthAcc hacc;
+            bool bad, cell;
+            int gx;
+            general_part<PHASE, NG>(s, ctl, tx, uy, strip, group, local_min, hacc, bad, cell, gx);
+            if (bad) atomicOr(&ctl->errors, 1u);
+            if (PHASE == 1) {
+                // the unit's first two and last two columns inside the grid
+                const int tx0 = s.x_org + tx * kTileX, ux0 = max(tx0, 0), ux1 = min(tx0 + kTileX, s.nx);
+                fold_unit_summary(hacc, cell, cell && gx < ux0 + 2, cell && gx >= ux1 - 2,
+                                  &s.usum[ctl->parity ^ 1][(size_t)uy * s.tiles_x + tx]);
+            } else {
+                // the minimum is exact in any order
+                for (int o = 16; o > 0; o >>= 1)
+                    local_min = fminf(local_min, __shfl_xor_sync(0xffffffffu, local_min, o));
+                if (lane == 0) atomicMin(&ctl->dt_bits, __float_as_uint(local_min));
+            }
+        }
+        int next = 0;
+        if (lane == 0) next = first_wave + atomicAdd(claim, 1);
+        t = __shfl_sync(0xffffffffu, next, 0);
     }
 }
 
@@ -1518,13 +1611,19 @@ static void launch_deep_any(const StepLaunch &L, cudaStream_t st)
     default: launch_deep<PHASE, 0>(L, st); break;
     }
 }
+template <int PHASE, int V>
+static void launch_general_v(const StepLaunch &L, cudaStream_t st)
+{
+    general_kernel<PHASE, general_ng(V)><<<L.grid, kGeneralThreads, 0, st>>>(L.scen, L.work, L.lists, L.cap,
+                                                                            L.claims + 2 + (PHASE - 1));
+}
 template <int PHASE>
 static void launch_general(const StepLaunch &L, cudaStream_t st)
 {
     switch (L.tiling.general) {
-    case 1: step_kernel<PHASE, general_ng(1)><<<L.grid, 128 * general_ng(1), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
-    case 2: step_kernel<PHASE, general_ng(2)><<<L.grid, 128 * general_ng(2), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
-    default: step_kernel<PHASE, general_ng(0)><<<L.grid, 128 * general_ng(0), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap); break;
+    case 1: launch_general_v<PHASE, 1>(L, st); break;
+    case 2: launch_general_v<PHASE, 2>(L, st); break;
+    default: launch_general_v<PHASE, 0>(L, st); break;
     }
 }
 
@@ -1546,7 +1645,7 @@ void launch_step_kernel(int k, const StepLaunch &L, cudaStream_t st)
 // phase 0 (initial dt) runs once per scenario: default tiling, the grid of L
 void launch_initial_dt(const StepLaunch &L, cudaStream_t st)
 {
-    step_kernel<0, general_ng(0)><<<L.grid, 128 * general_ng(0), 0, st>>>(L.scen, L.work, L.nwork, L.lists, L.cap);
+    initial_dt_kernel<general_ng(0)><<<L.grid, 128 * general_ng(0), 0, st>>>(L.scen, L.work, L.nwork);
 }
 
 void launch_lists_current(const StepLaunch &L, cudaStream_t st)
@@ -1577,10 +1676,10 @@ static cudaError_t preload(F *f)
 cudaError_t configure_step_kernels()
 {
     cudaError_t e;
-    if ((e = preload(step_kernel<0, general_ng(0)>)) || (e = preload(step_kernel<1, general_ng(0)>)) ||
-        (e = preload(step_kernel<1, general_ng(1)>)) || (e = preload(step_kernel<1, general_ng(2)>)) ||
-        (e = preload(step_kernel<2, general_ng(0)>)) || (e = preload(step_kernel<2, general_ng(1)>)) ||
-        (e = preload(step_kernel<2, general_ng(2)>)) || (e = preload(classify_kernel)))
+    if ((e = preload(initial_dt_kernel<general_ng(0)>)) || (e = preload(general_kernel<1, general_ng(0)>)) ||
+        (e = preload(general_kernel<1, general_ng(1)>)) || (e = preload(general_kernel<1, general_ng(2)>)) ||
+        (e = preload(general_kernel<2, general_ng(0)>)) || (e = preload(general_kernel<2, general_ng(1)>)) ||
+        (e = preload(general_kernel<2, general_ng(2)>)) || (e = preload(classify_kernel)))
         return e;
     if ((e = configure_deep<1, 0>()) || (e = configure_deep<1, 1>()) || (e = configure_deep<1, 2>()) ||
         (e = configure_deep<2, 0>()) || (e = configure_deep<2, 1>()) || (e = configure_deep<2, 2>()))
@@ -1593,9 +1692,9 @@ int step_blocks_per_sm(int v)
 {
     int n = 0;
     switch (v) {
-    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2, general_ng(1)>, 128 * general_ng(1), 0); break;
-    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2, general_ng(2)>, 128 * general_ng(2), 0); break;
-    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, step_kernel<2, general_ng(0)>, 128 * general_ng(0), 0); break;
+    case 1: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, general_kernel<2, general_ng(1)>, kGeneralThreads, 0); break;
+    case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, general_kernel<2, general_ng(2)>, kGeneralThreads, 0); break;
+    default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, general_kernel<2, general_ng(0)>, kGeneralThreads, 0); break;
     }
     return n;
 }

@@ -1103,11 +1103,12 @@ StepLaunch Batch::params() const
     L.claims = d_claims;
     L.cap = 2 * work_capacity;   // lists hold work units (two per work-list entry)
     L.tiling = tiling;
-    // general kernel: one CTA per SM more than are resident, striding over
-    // the list (measured at 4096^2 against 8 waves: 0.2965 against 0.3024 ms
-    // a step); deep kernels: persistent, one wave
+    // general kernel: persistent, one wave of warps that claim their tasks
+    // (4 strips x row groups per unit; 4 warps a CTA), no more CTAs than the
+    // tasks of a full list; deep kernels: persistent, one wave
     const int sms = device_sm_count();
-    L.grid = std::max(1, std::min(2 * work_capacity, sms * (std::max(1, step_blocks_per_sm(tiling.general)) + 1)));
+    L.grid = std::max(1, std::min(2 * work_capacity * general_ng(tiling.general),
+                                  sms * std::max(1, step_blocks_per_sm(tiling.general))));
     L.deep_grid[0] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(1, tiling.deep1))));
     L.deep_grid[1] = std::max(1, std::min(2 * work_capacity, sms * std::max(1, deep_blocks_per_sm(2, tiling.deep2))));
     L.classify_grid = std::max(1, std::min((2 * work_capacity + 127) / 128, 8 * device_sm_count()));

@@ -54,6 +54,7 @@ struct thy_server {
     std::deque<thy::Request> queue;
     std::vector<thy::Active *> slots;     // by batch slot
     bool members_changed = false;
+    bool alone = false;                   // the last chunk stepped one large request alone
     std::vector<char> selected;           // by batch slot: stepped in the last chunk (its work list)
     thy_server_stats stats{};
 };
@@ -216,7 +217,10 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
 {
     if (!S) return THY_ERR_INVALID;
     int rc;
-    if ((rc = admit(S))) return rc;
+    // while a large request runs alone, new requests wait in the queue: their
+    // set-up (uploads, Okada) would hold up its chunks, and none of them
+    // could be stepped before it ends
+    if (!S->alone && (rc = admit(S))) return rc;
     const int cap = S->b.capacity;
     bool state_changed = false, any_running = false;
     for (int i = 0; i < cap; i++) {
@@ -258,6 +262,7 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
     // chunk's work list).  Small requests are batched, a large one runs
     // alone, and no request's arithmetic changes.
     std::vector<char> sel(cap, 0);
+    S->alone = false;
     if (any_running) {
         // the request submitted first is always stepped (so that no request
         // waits behind a stream of smaller ones: the tail of time-to-result),
@@ -290,7 +295,7 @@ extern "C" int thy_server_progress(thy_server *S, int *active)
             const double cells = (double)s.nx * s.ny;
             bool step = !alone && (S->chunk_cells < 0 || taken < (double)S->chunk_cells);
             if (step && cells >= big) {
-                if (e.second == first) alone = true;
+                if (e.second == first) alone = S->alone = true;
                 else step = false;
             }
             if (step) taken += cells;
