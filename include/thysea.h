@@ -118,7 +118,7 @@ typedef struct thy_outputs {
 /* Warp tiling of the stepping kernels: a variant index 0..2 per kernel
    (row groups of warps per work unit: deep phase 1 {3, 2, 4} of 4 column
    strips, deep phase 2 {4, 2, 8} of 2 strips of column pairs, general
-   {2, 1, 4} of 4 strips; 0 is the default).  No result
+   {2, 1, 8} of 4 strips; 0 is the default).  No result
    depends on the tiling; the autotuner picks one per device and work size. */
 typedef struct thy_tiling {
     int deep1, deep2, general;

@@ -121,3 +121,7 @@ def test_head_to_head(refgpu, tmp_path, workload):
     assert abs(got_it - ref_it) <= 2
     if workload == "single_large_4096":
         assert cells * got_it / got_s > cells * ref_it / ref_s
+    else:
+        # the small grid: fixed per-run and per-step costs dominate both loops
+        # (graphs captured before the loop, short-chain tiling); at least 3x
+        assert got_s * 3.0 <= ref_s, (got_s, ref_s)

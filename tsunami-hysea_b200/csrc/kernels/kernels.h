@@ -56,7 +56,8 @@ struct Tiling {
 };
 // compute warps per CTA = 4 x deep_ng: deep phase 1 {3, 2, 4} (4 column strips
 // x that many row groups), deep phase 2 {2, 1, 4} (2 column strips of column
-// pairs x twice that many row groups); general {2, 1, 4} row groups
+// pairs x twice that many row groups); general {2, 1, 8} row groups (one warp
+// task per strip and row group; 8 groups of 2 rows for short chains)
 __host__ __device__ constexpr int deep_ng(int phase, int v)
 {
     return phase == 1 ? (v == 0 ? 3 : v == 1 ? 2 : 4) : (v == 0 ? 2 : v == 1 ? 1 : 4);
@@ -65,7 +66,7 @@ __host__ __device__ constexpr int deep_ng(int phase, int v)
 // two by its staging buffers; phase 2 (its lanes hold two columns) two, three
 // or one as its registers allow
 __host__ __device__ constexpr int deep_minb(int phase, int v) { return phase == 1 ? 2 : (v == 0 ? 2 : v == 1 ? 3 : 1); }
-__host__ __device__ constexpr int general_ng(int v) { return v == 0 ? 2 : v == 1 ? 1 : 4; }
+__host__ __device__ constexpr int general_ng(int v) { return v == 0 ? 2 : v == 1 ? 1 : 8; }
 
 // step.cu
 cudaError_t configure_step_kernels();

@@ -1084,13 +1084,15 @@ int Batch::chunk_for(long long steps) const { return (int)std::max(1ll, std::min
 int Batch::rebuild()
 {
     int rc;
-    if (!gexec) {
-        // grids for the capture need the capacity only; lists are reset by update()
-        if ((rc = capture())) return rc;
-    }
     if ((rc = update())) return rc;
-    if (!gexec && (rc = capture())) return rc;   // the work list grew past the capacity
-    return THY_OK;
+    // the graphs of the tiling the first chunk will take (the tuner's pick for
+    // the work now attached), a full chunk and one step, so that no capture
+    // falls into the time loop of a run whose work needs no tuning
+    bool sampling = false, known = false;
+    if ((rc = use_tiling(tuner_pick(tune_key(&known), &sampling)))) return rc;
+    for (const auto &g : graphs)
+        if (g.tiling == tiling && g.len == 1) return THY_OK;
+    return capture(1);
 }
 
 StepLaunch Batch::params() const

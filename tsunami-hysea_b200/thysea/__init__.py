@@ -214,7 +214,7 @@ def run(problem, max_steps: int = -1, snapshots: bool = True, series: bool = Tru
 
 # Warp tilings of the stepping kernels (thy_tiling): row groups per work unit
 # of each variant index, per kernel.  Results never depend on the tiling.
-TILING_GROUPS = {"deep1": (3, 2, 4), "deep2": (4, 2, 8), "general": (2, 1, 4)}
+TILING_GROUPS = {"deep1": (3, 2, 4), "deep2": (4, 2, 8), "general": (2, 1, 8)}
 
 
 def force_tiling(tiling=None):
