@@ -637,8 +637,19 @@ __device__ __forceinline__ float2 sel2(bool px, bool py, float2 a, float2 b)
 {
     return make_float2(px ? a.x : b.x, py ? a.y : b.y);
 }
-__device__ __forceinline__ float2 rcp_depth2(float2 h) { return make_float2(rcp_depth(h.x), rcp_depth(h.y)); }
+// Square roots of a pair (sqrt_ap per component, with its zero test: written
+// as a packed x * rsqrt(x) without it, the 16-warp deep phase 2 no longer
+// rounded like the other tilings), and 1/h and sqrt(h) of a cell pair from one
+// reciprocal square root per cell (deep cells: h > hpos >= 0)
 __device__ __forceinline__ float2 sqrt2(float2 h) { return make_float2(sqrt_ap(h.x), sqrt_ap(h.y)); }
+struct Depth2 {
+    float2 rh, sh;
+};
+__device__ __forceinline__ Depth2 depth2(float2 h)
+{
+    const float2 rs = make_float2(rsqrt_ap(h.x), rsqrt_ap(h.y));
+    return Depth2{mul2(rs, rs), make_float2(h.x == 0.f ? 0.f : __fmul_rn(h.x, rs.x), h.y == 0.f ? 0.f : __fmul_rn(h.y, rs.y))};
+}
 
 // two cells of a staged row (columns i, i + 1; i even)
 struct Cell2 {
@@ -658,6 +669,8 @@ __device__ __forceinline__ Cell2 staged_cell2(const float *st, int i)
 struct MomFlux2 {
     float2 m_x, m_y, p_x, p_y, lam;
 };
+// an edge's fluxes into one of its cells, as momentum_2s_* returns them (the
+// cell's update subtracts dt/area times their sum), and its wave-speed term
 struct Contrib2 {
     float2 a, b, lam;
 };
@@ -762,8 +775,8 @@ __device__ __forceinline__ void y_edge_deep2(const Cell2 &a, const Cell2 &b, flo
     const float2 jump = jump2<PLAIN>(a.e, b.e, a.D, b.D);
     MomFlux2 f;
     momentum_2s_y2(f, a.h, b.h, rha, rhb, sha, shb, a.qy, b.qy, a.qx, b.qx, jump, k);
-    lo = {neg2(f.m_x), neg2(f.m_y), f.lam};
-    hi = {neg2(f.p_x), neg2(f.p_y), f.lam};
+    lo = {f.m_x, f.m_y, f.lam};
+    hi = {f.p_x, f.p_y, f.lam};
 }
 
 // A deep work unit: unit code u = 2 * (work-list index) + half.
@@ -1097,13 +1110,15 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     const int r_first = prow0 + 1;                    // staged row of this warp's first output row
                     int i = r_first * kStageW + sc0;
                     Cell2 c = staged_cell2(stage, i);
-                    float2 rh_c = rcp_depth2(c.h), sh_c = sqrt2(c.h);
+                    const Depth2 fc = depth2(c.h);
+                    float2 rh_c = fc.rh, sh_c = fc.sh;
                     DeepRow rc = rows[r_first];
                     Contrib2 top;
                     {
                         const Cell2 a = staged_cell2(stage, i - kStageW);
                         Contrib2 dummy;
-                        y_edge_deep2<PLAIN>(a, c, rcp_depth2(a.h), sqrt2(a.h), rh_c, sh_c, rows[r_first - 1], rc, dummy, top);
+                        const Depth2 fa = depth2(a.h);
+                        y_edge_deep2<PLAIN>(a, c, fa.rh, fa.sh, rh_c, sh_c, rows[r_first - 1], rc, dummy, top);
                     }
                     float *out0 = d.out0, *out1 = d.out1;
                     int off = (yb + r_first - 1) * pitch + x0 - 4 + sc0;
@@ -1114,34 +1129,40 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                     for (int k = 0; k < PROWS; k++, i += kStageW, off += pitch) {
                         const DeepRow rn = rows[r_first + k + 1];
                         const Cell2 n = staged_cell2(stage, i + kStageW);
-                        const float2 rh_n = rcp_depth2(n.h), sh_n = sqrt2(n.h);
+                        const Depth2 fn = depth2(n.h);
+                        const float2 rh_n = fn.rh, sh_n = fn.sh;
                         // y edges below this row
                         Contrib2 below, next_top;
                         y_edge_deep2<PLAIN>(c, n, rh_c, sh_c, rh_n, sh_n, rc, rn, below, next_top);
                         // x edges left of column sc0 (its left neighbour, with its 1/h
                         // and sqrt h, is lane l-1's second column) and between sc0 and
                         // sc0 + 1 (lane 0 is halo: its left edge is not used)
-                        const float le = shup(c.e.y, 1), lD = shup(c.D.y, 1);
+                        const float le = shup(c.e.y, 1), lh = shup(c.h.y, 1);
                         const float lqx = shup(c.qx.y, 1), lqy = shup(c.qy.y, 1);
                         const float rhL = shup(rh_c.y, 1), shL = shup(sh_c.y, 1);
-                        const float2 jump = jump2<PLAIN>(make_float2(le, c.e.x), c.e, make_float2(lD, c.D.x), c.D);
+                        // (the left depth D only for the wet/dry tests of the jump)
+                        const float2 jump = PLAIN ? sub2(c.e, make_float2(le, c.e.x))
+                                                  : jump2<false>(make_float2(le, c.e.x), c.e,
+                                                                 make_float2(shup(c.D.y, 1), c.D.x), c.D);
                         MomFlux2 f;
-                        momentum_2s_x2(f, make_float2(le + lD, c.h.x), c.h, make_float2(rhL, rh_c.x), rh_c,
+                        momentum_2s_x2(f, make_float2(lh, c.h.x), c.h, make_float2(rhL, rh_c.x), rh_c,
                                        make_float2(shL, sh_c.x), sh_c, make_float2(lqx, c.qx.x), c.qx,
                                        make_float2(lqy, c.qy.x), c.qy, jump, XRowK{rc.m.y, rc.kdx});
                         // column sc0: right cell of the left edge, left cell of the
                         // middle edge; column sc0 + 1: right cell of the middle edge,
                         // left cell of lane l+1's left edge
-                        const Contrib2 xr = {neg2(f.p_x), neg2(f.p_y), f.lam};
-                        const Contrib2 xrr = {make_float2(-f.m_x.y, -shdn(f.m_x.x, 1)),
-                                              make_float2(-f.m_y.y, -shdn(f.m_y.x, 1)),
+                        const Contrib2 xr = {f.p_x, f.p_y, f.lam};
+                        const Contrib2 xrr = {make_float2(f.m_x.y, shdn(f.m_x.x, 1)),
+                                              make_float2(f.m_y.y, shdn(f.m_y.x, 1)),
                                               make_float2(f.lam.y, shdn(f.lam.x, 1))};
                         // momentum update; the dt bound as in the scalar path
                         const float2 lam = add2(add2(add2(xr.lam, xrr.lam), top.lam), below.lam);
                         const float2 w = mul2(lam, bc2(rc.kcfl));
                         const float wm = fmaxf(lam.x < kEps ? 0.f : w.x, lam.y < kEps ? 0.f : w.y);
                         if (out_lane) local_max = fmaxf(local_max, wm);
-                        const float2 val = bc2(rc.dtA);
+                        // q - dtA * (sum of the fluxes), bitwise the sum of the
+                        // negated fluxes times dtA (negation is exact)
+                        const float2 val = bc2(-rc.dtA);
                         const float2 qx = fma2(val, add2(add2(add2(xr.a, xrr.a), top.a), below.a), c.qx);
                         const float2 qy = fma2(val, add2(add2(add2(xr.b, xrr.b), top.b), below.b), c.qy);
                         if (out_lane) {
