@@ -753,6 +753,33 @@ def run_tilings(a, dist):
             "tilings": rows, "autotuner": {"pick": list(pick), "decided": decided, "tune_steps": tune_steps}}
 
 
+def run_launches(a, dist):
+    """Per-launch device times of the single-scenario workload (side --n):
+    --warmup steps in graphs, then --steps individually launched steps, each
+    launch timed with CUDA events.  The command the ncu summaries under
+    profiles/ capture (the launches of the individually launched steps come
+    after a known number of graph launches).  Not the headline line."""
+    import thysea
+    from thysea import synth
+
+    if thysea.device_count() == 0:
+        raise SystemExit("bench: no CUDA device")
+    thysea._ffi.lib().thy_set_device(dist.local)
+    p = synth.single_large(n=a.n, sim_time=3600.0)
+    sess = thysea.Session(thysea.Prepared(p))
+    sess.steps(a.warmup)
+    ms = sess.profile_launches(a.steps)
+    total, deep, dry = sess.tiles()
+    tiling = sess.tiling()
+    sess.close()
+    names = ("deep_phase1", "general_phase1", "classify", "deep_phase2", "general_phase2", "controller")
+    return {"metric": "ms per launch", "unit": "ms", "n_gpus": 1, "workload": "launches",
+            "config": {"workload": f"single_large {p.nx}x{p.ny}", "graph_steps": a.warmup, "launched_steps": a.steps,
+                       "tiling": {n: thysea.TILING_GROUPS[n][v] for n, v in zip(("deep1", "deep2", "general"), tiling)}},
+            "launch_ms": {n: round(v, 5) for n, v in zip(names, ms)},
+            "units": {"stepped": total, "deep": deep, "dry": dry}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -765,10 +792,12 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=400)
     ap.add_argument("--skip-e2e", action="store_true")
     ap.add_argument("--skip-cpu", action="store_true")
-    ap.add_argument("--workload", choices=["single", "batch", "mixed", "serving", "tilings"], default="single",
+    ap.add_argument("--workload", choices=["single", "batch", "mixed", "serving", "tilings", "launches"],
+                    default="single",
                     help="single: one 4096^2 scenario (the headline line); batch: 64 x 2048^2 on one "
                          "bathymetry; mixed: 32 scenarios of sides 256-4096; serving: Poisson requests; "
-                         "tilings: device time of each warp tiling (side --n)")
+                         "tilings: device time of each warp tiling (side --n); launches: per-launch times of "
+                         "--steps individually launched steps after --warmup steps in graphs (side --n)")
     ap.add_argument("--count", type=int, default=0, help="batch / mixed: number of scenarios (0: 64 / 32)")
     ap.add_argument("--rate", type=float, default=2.0, help="serving: requests per second")
     ap.add_argument("--duration", type=float, default=60.0, help="serving: seconds of arrivals")
@@ -786,6 +815,8 @@ def main():
             line = run_reference(a, dist)
         elif a.workload == "tilings":
             line = run_tilings(a, dist) if dist.rank == 0 else None
+        elif a.workload == "launches":
+            line = run_launches(a, dist) if dist.rank == 0 else None
         elif a.workload != "single":
             line = run_batched(a, dist)
         else:
