@@ -42,12 +42,14 @@ inline int tile_origin(int nx, bool periodic, int sp_left, int sp_right)
 }
 
 // Warp tilings of the stepping kernels, picked per workload by the autotuner
-// (runtime/tuner.cu).  A work unit is always kTileX x kHalfRows cells, each
-// of its four column strips marched by warps; a tiling says into how many row
-// groups a unit's rows are split (warps per CTA = 4 x groups) and how many
-// CTAs an SM keeps resident.  Every cell's arithmetic is the same under every
-// tiling (a warp recomputes the y edge above its first row from the same
-// inputs), so results do not depend on the tiling.  Variant 0 is the default.
+// (runtime/tuner.cu).  A work unit is always kTileX x kHalfRows cells, its
+// column strips marched by warps; a tiling says into how many row groups a
+// unit's rows are split (deep kernels: compute warps per CTA = 4 x groups of
+// the variant, and the CTAs an SM keeps resident follow; general kernel: one
+// warp task per strip and row group).  Every cell's arithmetic is the same
+// under every tiling (a warp recomputes the y edge above its first row from
+// the same inputs), so results do not depend on the tiling.  Variant 0 is the
+// default.
 constexpr int kTilingVariants = 3;
 struct Tiling {
     int deep1 = 0, deep2 = 0, general = 0;   // variant of deep phase 1, deep phase 2, the general kernel

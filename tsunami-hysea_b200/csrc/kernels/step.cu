@@ -1,14 +1,17 @@
 // Time-step kernels of the B200 stepper.
 //
-// One time step = five launches over a work list of (scenario, tile) items:
+// One time step = six launches over a work list of (scenario, tile) items:
 //   phase 1  mass fluxes -> new surface elevation, fused with the
 //            max-height / arrival-time diagnostics of the state the step
-//            starts from (src/GPU/Metrics.cu:23-77) and with the minimum
-//            water depth of each tile of the new state;
+//            starts from (src/GPU/Metrics.cu:23-77) and with the depth
+//            summary of each work unit of the new state (deep and general
+//            kernels, concurrent);
+//   classification of the units for the state phase 1 produced;
 //   phase 2  momentum fluxes with the phase-1 depths -> new discharges,
 //            sponge, shallow-water filter, Manning friction, local CFL dt,
-//            tile min -> one atomicMin per tile;
-//   control  one thread per scenario: time, next dt, events.
+//            one atomicMin per deep unit or general warp task (deep and
+//            general kernels, concurrent);
+//   control  one block per scenario: time, next dt, events, gauges.
 // Phases 1 and 2 are each a deep-water kernel and a general kernel.  A tile
 // is deep when every cell within two cells of it is deeper than hpos and it
 // is at least two cells from the boundaries and outside the sponge layers:
@@ -17,12 +20,14 @@
 // a fraction of the instructions and registers.  Both kernels evaluate the
 // same predicate on per-tile minimum depths that no launch of the phase
 // writes, so every tile is stepped by exactly one of them.
-// Phase 0 (the general template) computes the initial dt.
+// Phase 0 (the general kernel's arithmetic, one unit per CTA) computes the
+// initial dt.
 //
 // Row marching (general kernel): a unit is 4 column strips side by side, each
-// in two row groups of 8 rows, one warp per strip and group; each lane owns
-// one column and the warp marches down its rows keeping a five-row window of
-// its column in registers.  The y edge below the current
+// in row groups (a tiling: 1, 2 or 8), and each (strip, row group) is a task
+// of one warp, claimed independently of the others; each lane owns one
+// column and the warp marches down its rows keeping a five-row window of its
+// column in registers.  The y edge below the current
 // row needs nothing but that window; x edges take their left/right
 // neighbours from warp shuffles.  The 32 lanes cover 28 output columns plus
 // a two-column halo on each side (the x stencil reaches two cells), so the

@@ -102,10 +102,16 @@ static void complete(thy_server *S, int slot, int status)
     if (r.done) r.done(r.user, r.id, status, &st);
 }
 
-// Admits queued requests in order while they fit the budget and a slot.
+// Admits queued requests in order while they fit the budget and a slot: all
+// of them into an empty server, one a round otherwise (the set-up of each -
+// uploads, table, initial dt - holds the stepping thread, so a queue that
+// built up behind a large request joins one request a chunk, the first one
+// stepping as soon as it is set up).
 static int admit(thy_server *S)
 {
-    while (!S->queue.empty()) {
+    bool resident = false;
+    for (auto *a : S->slots) resident |= a != nullptr;
+    for (int n = 0; !S->queue.empty() && !(resident && n >= 1); n++) {
         Request &r = S->queue.front();
         if (S->in_use + r.bytes > S->budget && S->in_use > 0) break;   // wait for memory (an empty server admits anyway)
         int slot = -1;
