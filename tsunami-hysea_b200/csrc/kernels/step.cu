@@ -481,10 +481,10 @@ static_assert((SPLANE * 4) % 128 == 0 && (DPLANE * 4) % 128 == 0, "staged planes
 // row metrics of the current unit and the reduction scratch (one set per
 // buffer parity).
 constexpr size_t kNextBytes = 16 + 2 * 112;   // s_next[2], s_err, pad, s_unit[2]
-// A phase-1 staging buffer also receives the unit's packed row metrics, rows
+// A staging buffer also receives the unit's packed row metrics, rows
 // yb-2 .. yb+16 (a deep unit lies at least two rows inside the grid), copied
-// with the planes so that they arrive one unit ahead too; phase 2 derives its
-// row constants from them while its copies are in flight.
+// with the planes so that they arrive one unit ahead too; each phase derives
+// its row constants from them in shared memory.
 constexpr int kRawRows = kStageRows + 1;
 constexpr uint32_t kRawRowBytes = kRawRows * 16;
 __host__ __device__ constexpr size_t deep_raw_rows_offset(int phase)
@@ -493,7 +493,7 @@ __host__ __device__ constexpr size_t deep_raw_rows_offset(int phase)
 }
 __host__ __device__ constexpr size_t deep_stage_bytes(int phase)
 {
-    return deep_raw_rows_offset(phase) + (phase == 1 ? (kRawRowBytes + 127) / 128 * 128 : 0);   // 128-byte aligned
+    return deep_raw_rows_offset(phase) + (kRawRowBytes + 127) / 128 * 128;   // 128-byte aligned
 }
 struct DeepRow {
     float4 m;      // cos, ilcos, area, dlon (edge row)
@@ -852,10 +852,9 @@ __device__ __forceinline__ void deep_issue(const DeepUnit &d, float *stage, uint
         for (int k = 0; k < kNumMaps; k++) tmap_acquire(m + k);
         acq = m;
     }
-    mbar_expect_tx(bar, 4 * kStateBytes + (PHASE == 1 ? 3 * kDiagBytes + kRawRowBytes : 0));
-    if (PHASE == 1)
-        bulk_load(reinterpret_cast<unsigned char *>(stage) + deep_raw_rows_offset(PHASE), d.s->rowpack + d.yb - 2,
-                  kRawRowBytes, bar);
+    mbar_expect_tx(bar, 4 * kStateBytes + kRawRowBytes + (PHASE == 1 ? 3 * kDiagBytes : 0));
+    bulk_load(reinterpret_cast<unsigned char *>(stage) + deep_raw_rows_offset(PHASE), d.s->rowpack + d.yb - 2,
+              kRawRowBytes, bar);
     tma_load_2d(stage, m + me, d.x0 - 4, d.yb - 1, bar);
     tma_load_2d(stage + SPLANE, m + kMapDep, d.x0 - 4, d.yb - 1, bar);
     tma_load_2d(stage + 2 * SPLANE, m + kMapQx0 + p, d.x0 - 4, d.yb - 1, bar);
@@ -947,13 +946,15 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
             ScenarioCtl *ctl = d.ctl;
             const int x0 = d.x0, yb = d.yb;
             const float dt = d.dt;
+            if (!mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u)) s_err = 1;
+            const float4 *raw = reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE));
             if (PHASE == 2 && threadIdx.x < kStageRows) {
-                // row constants of the window with the unit's dt folded in,
-                // while the copies are in flight; staged row t is grid row
-                // yb - 1 + t
+                // row constants of the window with the unit's dt folded in, from
+                // the staged row metrics (row t of the window at t + 1; staged
+                // row t is grid row yb - 1 + t)
                 DeepRow r;
-                r.m = __ldg(d.rowpack + yb - 1 + threadIdx.x);
-                const float4 a = __ldg(d.rowpack + yb - 2 + threadIdx.x);   // the row above
+                r.m = raw[threadIdx.x + 1];
+                const float4 a = raw[threadIdx.x];   // the row above
                 r.icos = __frcp_rn(r.m.x);
                 r.dtA = __fdividef(dt, r.m.z);
                 r.kcfl = 1.f / (2.f * d.cfl * r.m.z);
@@ -963,11 +964,9 @@ __global__ void __launch_bounds__(128 * NG + 32, MINB) deep_kernel(const Scenari
                 r.y1 = make_float4(k.c01, k.li0, k.kdes0, k.kdes1);
                 rows[threadIdx.x] = r;
             }
-            if (!mbar_wait_bounded(&bars[buf], (phase_bits >> buf) & 1u)) s_err = 1;
             if (PHASE == 1 && threadIdx.x < kStageRows) {
-                // phase 1 row constants from the staged row metrics (row t of
-                // the window at t + 1): 1/cos for the y edges, dt/area
-                const float4 *raw = reinterpret_cast<const float4 *>(dsm + buf * SB + deep_raw_rows_offset(PHASE));
+                // phase 1 row constants from the staged row metrics: 1/cos for
+                // the y edges, dt/area
                 DeepRow r;
                 r.m = raw[threadIdx.x + 1];
                 r.icos = __frcp_rn(r.m.x);
